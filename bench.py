@@ -1,0 +1,342 @@
+"""Gradients/s of the WUST Helmholtz path on B200 (512^2 interior + 20-cell PML = 552^2, 256 TX).
+
+One step = one gradient: GPU assembly of the nine-point PML operator, block-LU
+factorization (552 Schur pages), forward solve of all 256 transmitters,
+receiver gather, source fit, misfit, adjoint solve, mass-stencil adjoint and
+FP64 gradient accumulation -- i.e. one wust_oracle call with two outputs.
+
+  value  inputs already resident in HBM (device pointers into the C ABI)
+  e2e    the same call with HOST buffers (medium, observations, gradient):
+         host<->device copies are inside the timed region
+Timing: W untimed warm-up steps, then K steps bracketed by barrier +
+cudaDeviceSynchronize, CUDA events on the solver stream, max over ranks.
+Every input (1.35 GB of Schur inverses, 0.6 GB fields per solve) is larger
+than the 126 MB L2, so no explicit flush is needed.
+
+``--impl reference`` times the reference's CPU path (sparse LU in FP64, the
+oracle port of HelmholtzSolver's cpu backend) on a bounded sample.
+Multi-GPU: replicas only (the Schur recursion does not shard); each rank runs
+its own gradient and ``value`` sums the ranks' gradients over the max time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = 552
+N_TX = 256
+FREQ = 1.2e6
+
+
+def flops_per_gradient(ny: int, nx: int, s: int) -> dict:
+    f_fac = 8.0 * (ny - 2) ** 3 * nx
+    f_apply = 2 * 8.0 * ny ** 2 * s * nx
+    return dict(factor=f_fac, apply=f_apply, gradient=f_fac + 2 * f_apply)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int = 0, period_ms: int = 200):
+        self.cmd = ["nvidia-smi", f"--id={index}",
+                    "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                    "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                    "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", f"-lms={period_ms}"]
+        self.lines: list[str] = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(self.cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=[], samples=0)
+        return dict(sm_mhz=float(np.median(sm)), sm_max_mhz=float(max(mx)), reasons=sorted(reasons),
+                    samples=len(sm))
+
+
+def make_problem(seed: int = 0):
+    from waveforminversionust_b200 import synthetic
+    return synthetic.config2(seed=seed, freqs=[FREQ])
+
+
+def cpu_reference_sample(p, n_solves: int = 8) -> dict:
+    """FP64 sparse-LU gradient timed on a bounded sample and extrapolated."""
+    from oracle import helmholtz_fp64 as o
+    ny, nx = p.shape
+    t0 = time.perf_counter()
+    s = o.HelmholtzSolverFP64(p.x_m, p.y_m, p.c_init, np.zeros(p.shape), FREQ, -1, 10.0, p.pml_m,
+                              dict(backend="cpu", stencil_bounds=(1400, 1700)), factor=False)
+    t1 = time.perf_counter()
+    lu = o.spla.splu(s.H)
+    t2 = time.perf_counter()
+    src = o.point_sources(p.tx_index, range(n_solves), ny, nx).reshape(ny * nx, n_solves, order="F")
+    lu.solve(src)
+    t3 = time.perf_counter()
+    lu.solve(src, trans="H")
+    t4 = time.perf_counter()
+    per_fwd = (t3 - t2) / n_solves
+    per_adj = (t4 - t3) / n_solves
+    t_grad = (t1 - t0) + (t2 - t1) + N_TX * (per_fwd + per_adj)
+    return dict(value=1.0 / t_grad, unit="gradients/s", cores=1, kind="port",
+                sample=(f"FP64 sparse LU (SciPy SuperLU, 1 thread) at {ny}x{nx}: assembly {t1 - t0:.2f} s + "
+                        f"factor {t2 - t1:.2f} s + {n_solves} forward and {n_solves} adjoint solves "
+                        f"({per_fwd * 1e3:.0f}/{per_adj * 1e3:.0f} ms each), extrapolated to {N_TX}+{N_TX} solves"),
+                seconds_per_gradient=t_grad)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    p = make_problem()
+    for _ in range(args.warmup):
+        cpu_reference_sample(p, n_solves=2)
+    vals = []
+    t0 = time.perf_counter()
+    last = None
+    for _ in range(args.steps):
+        last = cpu_reference_sample(p, n_solves=4)
+        vals.append(last["value"])
+    wall = time.perf_counter() - t0
+    v = float(np.mean(vals))
+    line = dict(impl="reference", metric="gradients_per_second", value=v, unit="gradients/s", n_gpus=args.gpus,
+                steps=args.steps, warmup=args.warmup, ms_per_step=1e3 / v, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="c128", data="synthetic",
+                config=dict(workload="config2 gradient: 552x552 grid (512^2 + 20-cell PML), dx 0.25 mm, 256 TX x "
+                                     "256 RX ring r = 55 mm, f = 1.2 MHz, breast-like phantom", global_batch=N_TX),
+                cpu_baseline=dict(value=v, unit="gradients/s", cores=1, kind="port", sample=last["sample"]),
+                e2e=dict(value=v, unit="gradients/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+                wall_seconds=wall)
+    print(json.dumps(line), flush=True)
+
+
+def generate_observations(p, solver_cls, torch):
+    """Observed pressure from the refined GPU solver on the true model."""
+    from waveforminversionust_b200.objective import Observations
+    ny, nx = p.shape
+    s = solver_cls(p.x_m, p.y_m, p.c_true, None, FREQ, -1, 10.0, p.pml_m,
+                   dict(backend="gpu", stencil_bounds=(1400, 1700)), precision="c64-refined", max_sources=N_TX)
+    src = torch.zeros((N_TX, nx, ny), dtype=torch.complex64, device="cuda")
+    lin = torch.as_tensor(p.tx_index - 1, device="cuda")
+    src.view(N_TX, -1)[torch.arange(N_TX, device="cuda"), lin] = 1
+    u = s.solve(src.permute(2, 1, 0))
+    uf = u.permute(2, 1, 0).reshape(N_TX, -1)
+    rx = torch.as_tensor(p.rx_index - 1, device="cuda")
+    Y = uf[:, rx].cpu().numpy()[:, :, None]
+    s.close()
+    del src, u, uf
+    mask = np.ones((N_TX, p.rx_index.size, 1), bool)
+    return Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, [FREQ], Y, mask)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="c64-refined")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variants", default="c64", help="extra precision profiles timed beside the headline")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    from waveforminversionust_b200 import _lib
+    from waveforminversionust_b200.objective import default_config
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    lib = _lib.load()
+
+    p = make_problem(seed=rank)
+    ny, nx = p.shape
+    obs = generate_observations(p, HelmholtzSolver, torch)
+    fl = flops_per_gradient(ny, nx, N_TX)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def measure(precision: str, with_e2e: bool):
+        cfg = default_config(pml_m=p.pml_m, precision=precision, source_batch_size=N_TX)
+        solver = HelmholtzSolver(p.x_m, p.y_m, p.c_init, None, FREQ, -1, 10.0, p.pml_m,
+                                 dict(backend="gpu", stencil_bounds=(1400, 1700)), precision=precision,
+                                 max_sources=N_TX, stream=stream)
+        h = C.c_void_p(solver.handle)
+        c_dev = torch.as_tensor(np.asfortranarray(p.c_init).T.copy(), device="cuda")   # (nx, ny) == col-major
+        tx_dev = torch.as_tensor(obs.tx_index.astype(np.int32), device="cuda")
+        rx_dev = torch.as_tensor(obs.rx_index.astype(np.int32), device="cuda")
+        Y_dev = torch.as_tensor(np.asfortranarray(obs.Y[:, :, 0]).T.astype(np.complex64).copy(), device="cuda")
+        m_dev = torch.as_tensor(np.asfortranarray(obs.mask[:, :, 0]).T.astype(np.uint8).copy(), device="cuda")
+        g_dev = torch.empty((nx, ny), dtype=torch.float64, device="cuda")
+        loss = C.c_double()
+
+        def step_device():
+            _lib.check(lib.wust_solver_refactor(h, C.c_void_p(c_dev.data_ptr()), None, C.c_double(FREQ)))
+            _lib.check(lib.wust_solver_oracle(h, C.c_void_p(tx_dev.data_ptr()), N_TX, C.c_void_p(rx_dev.data_ptr()),
+                                              obs.n_rx, C.c_void_p(Y_dev.data_ptr()), C.c_void_p(m_dev.data_ptr()),
+                                              N_TX, _lib.NEED_GRADIENT, C.byref(loss), C.c_void_p(g_dev.data_ptr())))
+
+        # host buffers for e2e (pinned, as a caller would keep them)
+        c_h = torch.as_tensor(np.asfortranarray(p.c_init).T.copy()).pin_memory()
+        tx_h = np.ascontiguousarray(obs.tx_index.astype(np.int32))
+        rx_h = np.ascontiguousarray(obs.rx_index.astype(np.int32))
+        Y_h = torch.as_tensor(np.asfortranarray(obs.Y[:, :, 0]).T.astype(np.complex64).copy()).pin_memory()
+        m_h = torch.as_tensor(np.asfortranarray(obs.mask[:, :, 0]).T.astype(np.uint8).copy()).pin_memory()
+        g_h = torch.empty((nx, ny), dtype=torch.float64).pin_memory()
+
+        def step_host():
+            _lib.check(lib.wust_solver_refactor(h, C.c_void_p(c_h.data_ptr()), None, C.c_double(FREQ)))
+            _lib.check(lib.wust_solver_oracle(h, tx_h.ctypes.data_as(C.c_void_p), N_TX,
+                                              rx_h.ctypes.data_as(C.c_void_p), obs.n_rx,
+                                              C.c_void_p(Y_h.data_ptr()), C.c_void_p(m_h.data_ptr()), N_TX,
+                                              _lib.NEED_GRADIENT, C.byref(loss), C.c_void_p(g_h.data_ptr())))
+
+        for _ in range(args.warmup):
+            step_device()
+        barrier()
+        fac_ms, launches = [], 0
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            barrier()
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step_device()
+                fac_ms.append(solver.factor_seconds * 1e3)
+                launches += solver.stats()["kernel_launches"] + 1
+            ev1.record(stream)
+            barrier()
+        dev_ms = max_over_ranks(ev0.elapsed_time(ev1))
+        stats = solver.stats()
+        res = dict(ms_per_step=dev_ms / args.steps, value=world * args.steps / (dev_ms * 1e-3),
+                   factor_ms=float(np.mean(fac_ms)), launches_per_step=launches / args.steps,
+                   refine_iters=stats["refine_iters"], final_residual=stats["final_residual"],
+                   loss=loss.value, clocks=clk.summary())
+        if with_e2e:
+            for _ in range(2):
+                step_host()
+            barrier()
+            ev0.record(stream)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                step_host()
+            ev1.record(stream)
+            barrier()
+            e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+            N = ny * nx
+            h2d = N * 8 + 4 * (obs.n_tx + obs.n_rx) + obs.n_tx * obs.n_rx * (8 + 1) + N * 4
+            d2h = N * 8 + obs.n_tx * 8
+            res["e2e"] = dict(value=world * args.steps / (e2e_ms * 1e-3), unit="gradients/s",
+                              h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
+                              wall_ms_per_step=(time.perf_counter() - t0) * 1e3 / args.steps)
+        solver.close()
+        return res
+
+    head = measure(args.precision, with_e2e=True)
+    variants = {}
+    for v in [x for x in args.variants.split(",") if x and x != args.precision]:
+        variants[v] = measure(v, with_e2e=False)
+        variants[v].pop("clocks", None)
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak_tf = float(peaks.get("bf16_tflops", 1590.0))
+    fac_tflops = fl["factor"] / (head["factor_ms"] * 1e-3) / 1e12
+    roofline = dict(kernel="factor_kernel (Schur recursion + Gauss-Jordan inverses)", bound="tensor",
+                    achieved=fac_tflops, peak=peak_tf, unit="TFLOP/s", frac=fac_tflops / peak_tf,
+                    peak_source="MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1590 TFLOP/s",
+                    traffic=None, algorithmic_flop_per_launch=fl["factor"])
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_sample(p, n_solves=8)
+    line = dict(metric="gradients_per_second", value=head["value"], unit="gradients/s", n_gpus=world,
+                steps=args.steps, warmup=args.warmup, ms_per_step=head["ms_per_step"], higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="c64+c128-refine" if args.precision != "c64" else "c64",
+                data="synthetic",
+                config=dict(workload="config2 gradient: 552x552 grid (512^2 + 20-cell PML), dx 0.25 mm, 256 TX x "
+                                     "256 RX ring r = 55 mm, f = 1.2 MHz, breast-like phantom",
+                            global_batch=N_TX * world, precision=args.precision, parallelism=f"replicas{world}",
+                            l2="inputs larger than L2 (invT 1.35 GB, fields 0.62 GB)"),
+                e2e=head["e2e"], gpu_launches=int(round(head["launches_per_step"] * args.steps)),
+                roofline=roofline, clocks=head["clocks"],
+                detail=dict(factor_ms=head["factor_ms"], refine_iters=head["refine_iters"],
+                            final_relative_residual=head["final_residual"], flops=fl, variants=variants))
+    if cpu:
+        line["cpu_baseline"] = dict(value=cpu["value"], unit="gradients/s", cores=cpu["cores"], kind=cpu["kind"],
+                                    sample=cpu["sample"])
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,191 @@
+/*
+ * wust_b200.h -- C ABI of the B200 (sm_100a) Helmholtz gradient library.
+ *
+ * The library replaces the GPU path of WaveformInversionUST's HelmholtzSolver
+ * (Runtime/solver/HelmholtzSolver.m) and its two MEX kernels
+ * (Runtime/solver/decompBlockLU.cu, Runtime/solver/applyBlockLU.cu), plus the
+ * per-frequency misfit/gradient (Runtime/matlab/wust_oracle.m) and the
+ * directional curvature (Runtime/matlab/directional_curvature.m).
+ *
+ * Conventions (identical to the reference):
+ *   - 2-D grids are column-major [y, x] (y fastest), Ny rows by Nx columns;
+ *     RHS stacks are [y, x, source].  Linear grid indices are 1-based
+ *     (MATLAB sub2ind), as in obs.tx_index / obs.rx_index.
+ *   - Complex numbers are interleaved (re, im).
+ *   - Every call returns a wust_status; wust_status_id() maps it to the
+ *     reference's error identifier and wust_last_error() gives the message
+ *     of the last failing call on the calling thread.
+ *   - Unless stated otherwise, array arguments may be host or device memory;
+ *     the library detects which (cudaPointerGetAttributes) and stages host
+ *     buffers through its own device copies.  The legacy MEX-equivalent
+ *     entry points take device pointers only, like mxGPUArray data.
+ *   - No entry point falls back to the CPU: without a usable CUDA device
+ *     every compute call fails with WUST_ERR_CUDA.
+ */
+#ifndef WUST_B200_H
+#define WUST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float re, im; } wust_c64;
+typedef struct { double re, im; } wust_c128;
+
+/* Status codes; names mirror the reference ids (block_lu_mex_utils.h:37-159,
+ * wust_oracle.m:55-80). */
+enum wust_status {
+    WUST_OK = 0,
+    WUST_ERR_INVALID_INPUT = 1,            /* WUST:InvalidInput */
+    WUST_ERR_INVALID_OUTPUT = 2,           /* WUST:InvalidOutput */
+    WUST_ERR_CUDA = 3,                     /* WUST:CUDAError */
+    WUST_ERR_CUBLAS = 4,                   /* WUST:CUBLASError (id kept; no library GEMM is used) */
+    WUST_ERR_CUSOLVER = 5,                 /* WUST:CUSOLVERError (id kept; no library solver is used) */
+    WUST_ERR_SINGULAR_SCHUR_BLOCK = 6,     /* WUST:SingularSchurBlock */
+    WUST_ERR_INVALID_SOLVER_ARGUMENT = 7,  /* WUST:InvalidSolverArgument */
+    WUST_ERR_RESOURCE_CLEANUP = 8,         /* WUST:ResourceCleanup */
+    WUST_ERR_RUNTIME = 9,                  /* WUST:RuntimeError */
+    WUST_ERR_NUMERICAL_FAILURE = 10,       /* WUST:NumericalFailure */
+    WUST_ERR_DEVICE_TIMEOUT = 11,          /* WUST:DeviceTimeout: a bounded device-side wait expired */
+    WUST_ERR_NOT_CONVERGED = 12            /* WUST:RefinementNotConverged */
+};
+
+/* Precision profiles of the solver. */
+enum wust_precision {
+    WUST_PRECISION_C64 = 0,          /* plain complex-single block LU: the reference algorithm */
+    WUST_PRECISION_C64_REFINED = 1,  /* c64 block LU + FP64-residual iterative refinement */
+    WUST_PRECISION_BF16_REFINED = 2, /* BF16 tensor-core Schur/solve GEMMs + FP64 refinement */
+    WUST_PRECISION_TF32_REFINED = 3  /* TF32 tensor-core Schur/solve GEMMs + FP64 refinement */
+};
+
+/* Oracle request flags (wust_oracle.m:5-6: nargout selects the work). */
+enum wust_oracle_flags {
+    WUST_NEED_GRADIENT = 1,   /* adjoint solve + slowness gradient */
+    WUST_RETAIN_STATE = 2     /* keep forward fields and source scales for wust_solver_curvature */
+};
+
+const char *wust_status_id(int status);
+const char *wust_last_error(void);
+int wust_version(int *major, int *minor, int *patch);
+
+/* ------------------------------------------------------------------------
+ * Legacy MEX-equivalent entry points.  Device pointers, complex single.
+ * ------------------------------------------------------------------------ */
+
+/* Replaces `invT = decompBlockLU(Ld,Ll,Lu,Dd,Dl,Du,Ud,Ul,Uu)`
+ * (Runtime/solver/decompBlockLU.cu:173-396; call site HelmholtzSolver.m:167-168).
+ * Shapes (column-major): Ld, Ud: Ny x (Nx-1); Ll, Lu, Ul, Uu: (Ny-1) x (Nx-1);
+ * Dd: Ny x Nx; Dl, Du: (Ny-1) x Nx.  Ny >= 3, Nx >= 2, Ny*Nx < 2^31.
+ * invT: caller-allocated Ny x Ny x Nx; every page's border rows and columns
+ * are written as zero and its interior holds inv(T_j interior).
+ * total_gpu_ms (nullable) receives the device time like the optional timing
+ * struct's total_gpu_ms field (decompBlockLU.cu:379-388).  stream may be NULL
+ * (legacy default stream).  The call is synchronous, like the MEX. */
+int wust_decomp_block_lu(const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 *Lu,
+                         const wust_c64 *Dd, const wust_c64 *Dl, const wust_c64 *Du,
+                         const wust_c64 *Ud, const wust_c64 *Ul, const wust_c64 *Uu,
+                         int Ny, int Nx, wust_c64 *invT, float *total_gpu_ms, void *stream);
+
+/* Replaces `u = applyBlockLU(SRC,Ld,Ll,Lu,Ud,Ul,Uu,invT,adjoint)`
+ * (Runtime/solver/applyBlockLU.cu:291-481; call site HelmholtzSolver.m:182-184).
+ * src, u: Ny x Nx x n_src; u is caller-allocated and fully overwritten.
+ * adjoint != 0 solves H^H u = src with the reference's sweep order. */
+int wust_apply_block_lu(const wust_c64 *src, int Ny, int Nx, int n_src,
+                        const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 *Lu,
+                        const wust_c64 *Ud, const wust_c64 *Ul, const wust_c64 *Uu,
+                        const wust_c64 *invT, int adjoint, wust_c64 *u, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Solver object: one HelmholtzSolver instance (model + frequency).
+ * ------------------------------------------------------------------------ */
+
+typedef struct wust_solver wust_solver;
+
+/* Constructor arguments of HelmholtzSolver(x, y, vel, atten, f,
+ * signConvention, a0, L_PML, options) (HelmholtzSolver.m:32-52). */
+typedef struct {
+    int ny, nx;                    /* grid size including PML */
+    const double *x_m;             /* host, nx increasing uniform samples */
+    const double *y_m;             /* host, ny increasing uniform samples */
+    double frequency_hz;
+    double sign_convention;        /* wust_oracle passes -1 */
+    double pml_strength;           /* a0 */
+    double pml_m;                  /* L_PML */
+    double stencil_vmin, stencil_vmax;   /* options.stencil_bounds */
+    int dispersion;                /* 0: continuum; 1: kwave-ldr9 (needs the two below) */
+    double time_step_s, reference_speed_mps;
+    int precision;                 /* enum wust_precision */
+    int refine_max_iters;          /* refined profiles: max refinement solves (0 -> 8) */
+    double refine_tol;             /* refined profiles: relative FP64 residual target (0 -> 1e-5) */
+    int max_sources;               /* largest RHS batch the object will see (0 -> 256) */
+} wust_solver_options;
+
+/* Assemble the nine-point PML operator on the GPU and factorize it.
+ * vel, atten: ny x nx (atten may be NULL = zero).  stream may be NULL. */
+int wust_solver_create(wust_solver **out, const wust_solver_options *options,
+                       const double *vel, const double *atten, void *stream);
+/* Re-assemble and re-factorize for a new medium and/or frequency on the
+ * same grid, reusing all device buffers (one NCG step = one refactor). */
+int wust_solver_refactor(wust_solver *s, const double *vel, const double *atten,
+                         double frequency_hz);
+int wust_solver_destroy(wust_solver *s);
+
+/* Wall/device timings of the last construction (HelmholtzSolver.m:15-16). */
+int wust_solver_timings(const wust_solver *s, double *assembly_ms, double *factor_ms);
+/* Stencil mass weights b, d, e (obj.massD / obj.massE; stencilOptParams.m). */
+int wust_solver_stencil(const wust_solver *s, double *b, double *d, double *e);
+
+/* Device views of the factor blocks (HelmholtzSolver.m:18-24 properties).
+ * names: "Dd","Dl","Du","Ld","Ll","Lu","Ud","Ul","Uu","invT","mult".
+ * The pointer stays owned by the solver. */
+int wust_solver_block(const wust_solver *s, const char *name, const void **device_ptr,
+                      int *rows, int *cols, int *pages);
+
+/* solve(src, adjoint) (HelmholtzSolver.m:174-203): out = H^{-1} src or
+ * H^{-H} src for n_src right-hand sides; virt (nullable) receives the
+ * virtual sources mult .* out. */
+int wust_solver_solve(wust_solver *s, const wust_c64 *src, int n_src, int adjoint,
+                      wust_c64 *out, wust_c64 *virt);
+
+/* massApply(v, adjoint) (HelmholtzSolver.m:205-220). */
+int wust_solver_mass_apply(wust_solver *s, const wust_c64 *v, int n, int adjoint, wust_c64 *out);
+
+/* [loss, gradient, cache] = wust_oracle(c, obs, fi, cfg) for the solver's
+ * model and frequency (wust_oracle.m:1-86).
+ * tx_index, rx_index: 1-based linear grid indices (host or device, int32).
+ * Y: n_tx x n_rx complex single observations of this frequency; mask: n_tx x
+ * n_rx bytes (0/1).  source_batch_size <= 0 means all transmitters at once.
+ * gradient (nullable unless WUST_NEED_GRADIENT): ny x nx double. */
+int wust_solver_oracle(wust_solver *s, const int32_t *tx_index, int n_tx,
+                       const int32_t *rx_index, int n_rx,
+                       const wust_c64 *Y, const uint8_t *mask,
+                       int source_batch_size, int flags,
+                       double *loss, double *gradient);
+
+/* directional_curvature(state, direction, rx_index, mask) on the state kept
+ * by the last oracle call with WUST_RETAIN_STATE
+ * (directional_curvature.m:1-26).  direction: ny x nx double. */
+int wust_solver_curvature(wust_solver *s, const double *direction, double *curvature);
+
+/* Counters of the last solve/oracle call: correction solves of the last
+ * refined solve, its final relative FP64 residual |b - Hx| / |b| and forward
+ * error estimate (refined profiles; -1 otherwise), and the number of kernel
+ * launches the call issued. */
+int wust_solver_stats(const wust_solver *s, int *refine_iters, double *final_residual,
+                      double *error_estimate, long long *kernel_launches);
+
+/* Self-test of the bounded device-side wait used by the persistent kernels
+ * (no counterpart in the reference, whose MEX calls are synchronous library
+ * calls): one CTA waits at a grid barrier that can never fill; the wait must
+ * give up after timeout_ms, leave the context usable and report its site.
+ * Returns WUST_ERR_DEVICE_TIMEOUT when the timeout path works. */
+int wust_selftest_barrier_timeout(int timeout_ms, int *site);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WUST_B200_H */

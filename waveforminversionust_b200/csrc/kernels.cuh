@@ -1,0 +1,85 @@
+// Host-side launchers shared between the translation units of libwust_b200.
+#pragma once
+
+#include "common.cuh"
+
+namespace wust {
+
+enum SweepMode { SWEEP_F1 = 0, SWEEP_F2 = 1, SWEEP_A1 = 2, SWEEP_A2 = 3 };
+
+// ---- factor.cu -------------------------------------------------------------
+size_t factor_scratch_bytes(int ny);
+// host_status (nullable, int[3]): {1+bad page, pivot, barrier timeout site};
+// when non-null the call synchronizes the stream.
+void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t scratch_bytes,
+                   cudaStream_t stream, double timeout_s, int *host_status);
+int barrier_selftest(double timeout_s, int *site_out);
+
+// ---- sweep.cu --------------------------------------------------------------
+// u (ny*nx*S) is overwritten; tmp needs ny*S elements.
+void sweep_solve(const Coefs<float2> &co, const float2 *invT, const SrcView &src, int S, bool adjoint,
+                 float2 *u, float2 *tmp, cudaStream_t st);
+
+// ---- assemble.cu -----------------------------------------------------------
+struct AssemblyInput {
+    int ny, nx;
+    double f, sgn, a0, L;
+    double xmin, xmax, ymin, ymax;
+    double h, g;
+    double b, d, e;
+    int ldr9;
+    double dt, cr;
+};
+// vel, atten: device ny*nx (atten may be null). Outputs: 9 c128 + 9 c64
+// blocks in the reference layout and the c128 virtual-source multiplier.
+void assemble_launch(const AssemblyInput &in, const double *vel, const double *atten,
+                     const double *ex_col, const double *ey_row,   // device, 2*(n-1)+1 imaginary parts
+                     double2 *const co128[9], float2 *const co64[9], double2 *mult, int *status,
+                     cudaStream_t st);
+void stencil_opt_params(double vmin, double vmax, double f, double h, double g, double *b, double *d,
+                        double *e);
+
+// ---- objective.cu ----------------------------------------------------------
+struct FitParams {
+    const float2 *u;          // forward fields [ny, nx, nb]
+    const double2 *u64;       // nullable: FP64 refined fields (gathered instead of u)
+    const int32_t *rx_lin;    // 0-based
+    const float2 *Y;          // [n_tx, n_rx] observations of this frequency
+    const uint8_t *mask;      // [n_tx, n_rx]
+    int n_tx, n_rx, first_tx, nb, ny, nx;
+    float2 *residual;         // [n_rx, nb] adjoint sources (c64)
+    double2 *scale;           // [nb]
+    double *loss_per_src;     // [nb]
+    int *status;              // [0] = 1 + first failing source
+};
+void fit_launch(const FitParams &p, cudaStream_t st);
+
+// g(y,x) += sum_s -Re(conj(scale_s * mult * u_s) * (M^T lam_s))   (wust_oracle.m:66-68)
+void gradient_launch(const float2 *u, const float2 *lam, const double2 *mult, const double2 *scale, int ny,
+                     int nx, int nb, double d, double e, double *grad, cudaStream_t st);
+// out = massApply(v, adjoint) for plain fields (HelmholtzSolver.m:205-220)
+void mass_apply_launch(const float2 *v, float2 *out, int ny, int nx, int n, double d, double e, bool adjoint,
+                       cudaStream_t st);
+// out = massApply(mult .* u .* direction, false): curvature sources
+void curvature_source_launch(const float2 *u, const double2 *mult, const double *direction, float2 *out, int ny,
+                             int nx, int nb, double d, double e, cudaStream_t st);
+// per-source sum |u(rx) * scale * mask|^2 -> out[nb]
+void curvature_reduce_launch(const float2 *u, const int32_t *rx_lin, const uint8_t *mask, const double2 *scale,
+                             int n_tx, int n_rx, int first_tx, int nb, int ny, int nx, double *out,
+                             cudaStream_t st);
+// virt = mult .* u
+void virtual_source_launch(const float2 *u, const double2 *mult, float2 *virt, int ny, int nx, int n,
+                           cudaStream_t st);
+
+// ---- refine.cu -------------------------------------------------------------
+// r = b - H x (or H^H) in FP64 on rows y in [1, ny-2]; r64 -> c64 copy for the
+// correction solve; per-source squared norms of r and of b.
+void residual_launch(const Coefs<double2> &co, const SrcView &b, const double2 *x, int S, bool adjoint,
+                     float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st);
+void promote_launch(const float2 *u, double2 *x, size_t n, cudaStream_t st);          // x = u
+// x += d per source plane; per-source squared norms of d and of the new x
+void accumulate_launch(const float2 *d, double2 *x, size_t plane, int S, double *dnorm2, double *xnorm2,
+                       cudaStream_t st);
+void demote_launch(const double2 *x, float2 *u, size_t n, cudaStream_t st);           // u = x
+
+}  // namespace wust

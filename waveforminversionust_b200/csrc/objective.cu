@@ -1,0 +1,259 @@
+// Per-frequency objective pieces on the GPU (Runtime/matlab/wust_oracle.m,
+// Runtime/matlab/directional_curvature.m, HelmholtzSolver.massApply):
+//   fit_kernel          receiver gather, masked source fit a = p^H d / p^H p,
+//                       residual, 0.5 |r|^2 (wust_oracle.m:43-61), FP64 sums
+//   gradient_kernel     g += sum_s -Re(conj(a_s v_s) .* M^T lam_s), with the
+//                       mass stencil's border zeroed first (wust_oracle.m:66-68,
+//                       HelmholtzSolver.m:211-215); FP64 accumulation over s
+//   mass_apply_kernel   massApply forward/adjoint (HelmholtzSolver.m:205-220)
+//   curvature kernels   massApply(v .* direction) and sum |a u(rx) mask|^2
+//                       (directional_curvature.m:12-20)
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace wust {
+
+// ---------------------------------------------------------------------------
+// block reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int NT>
+__device__ double block_sum(double v, double *sh) {
+    v = warp_sum(v);
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double t = (threadIdx.x < NT / 32) ? sh[threadIdx.x] : 0.0;
+    if (w == 0) t = warp_sum(t);
+    if (threadIdx.x == 0) sh[0] = t;
+    __syncthreads();
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+constexpr int FIT_THREADS = 256;
+
+__global__ void __launch_bounds__(FIT_THREADS) fit_kernel(FitParams p) {
+    __shared__ double sh[FIT_THREADS / 32];
+    const int s = blockIdx.x;
+    const int t = p.first_tx + s;
+    const size_t off = (size_t)p.ny * p.nx * s;
+    // The misfit residual is a small difference of the field at the receivers,
+    // so refined solves are gathered from their FP64 accumulator.
+    auto field = [&](int r) -> double2 {
+        const int32_t q = p.rx_lin[r];
+        return p.u64 ? p.u64[off + q] : z_from(p.u[off + q]);
+    };
+    double den = 0, nre = 0, nim = 0;
+    for (int r = threadIdx.x; r < p.n_rx; r += FIT_THREADS) {
+        const double m = p.mask[t + (size_t)p.n_tx * r] ? 1.0 : 0.0;
+        const double2 pm = zscale(m, field(r));
+        const double2 dm = zscale(m, z_from(p.Y[t + (size_t)p.n_tx * r]));
+        den += zabs2(pm);
+        nre += pm.x * dm.x + pm.y * dm.y;    // conj(pm) * dm
+        nim += pm.x * dm.y - pm.y * dm.x;
+    }
+    den = block_sum<FIT_THREADS>(den, sh);
+    nre = block_sum<FIT_THREADS>(nre, sh);
+    nim = block_sum<FIT_THREADS>(nim, sh);
+    const bool ok = isfinite(den) && den > 2.2250738585072014e-308 && isfinite(nre) && isfinite(nim);
+    const double2 a = ok ? make_double2(nre / den, nim / den) : make_double2(0.0, 0.0);
+    if (!ok || !isfinite(a.x) || !isfinite(a.y)) {
+        if (threadIdx.x == 0) atomicCAS(p.status, 0, t + 1);
+    }
+    double loss = 0;
+    for (int r = threadIdx.x; r < p.n_rx; r += FIT_THREADS) {
+        const double m = p.mask[t + (size_t)p.n_tx * r] ? 1.0 : 0.0;
+        const double2 pm = zscale(m, field(r));
+        const double2 dm = zscale(m, z_from(p.Y[t + (size_t)p.n_tx * r]));
+        const double2 res = zscale(m, zsub(zmul(pm, a), dm));
+        loss += zabs2(res);
+        p.residual[r + (size_t)p.n_rx * s] = c_from(res);
+    }
+    loss = block_sum<FIT_THREADS>(loss, sh);
+    if (threadIdx.x == 0) {
+        p.scale[s] = a;
+        p.loss_per_src[s] = 0.5 * loss;
+    }
+}
+
+void fit_launch(const FitParams &p, cudaStream_t st) {
+    fit_kernel<<<p.nb, FIT_THREADS, 0, st>>>(p);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 mass stencil tiles.  The kernel is symmetric, so convn and correlation
+// coincide: w = [e/4 d/4 e/4; d/4 1-d-e d/4; e/4 d/4 e/4].
+// ---------------------------------------------------------------------------
+constexpr int TY = 32, TX = 8;
+
+__device__ __forceinline__ double mass_w(int dy, int dx, double d, double e) {
+    const int a = (dy != 0) + (dx != 0);
+    return a == 0 ? 1.0 - d - e : (a == 1 ? d / 4 : e / 4);
+}
+
+__device__ __forceinline__ bool on_ring(int y, int x, int ny, int nx) {
+    return y == 0 || x == 0 || y == ny - 1 || x == nx - 1;
+}
+
+__global__ void __launch_bounds__(TY * TX) gradient_kernel(const float2 *u, const float2 *lam, const double2 *mult,
+                                                           const double2 *scale, int ny, int nx, int nb, double d,
+                                                           double e, double *grad) {
+    __shared__ float2 L[TX + 2][TY + 2];
+    const int ty = threadIdx.x % TY, tx = threadIdx.x / TY;
+    const int y0 = blockIdx.x * TY, x0 = blockIdx.y * TX;
+    const int y = y0 + ty, x = x0 + tx;
+    const bool inside = (y < ny && x < nx);
+    const size_t idx = (size_t)y + (size_t)ny * x;
+    const double2 m = inside ? mult[idx] : make_double2(0.0, 0.0);
+    double w[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) w[a][b] = mass_w(a - 1, b - 1, d, e);
+    double acc = 0;
+    const size_t fs = (size_t)ny * nx;
+    for (int s = 0; s < nb; ++s) {
+        const float2 *ls = lam + fs * s;
+        for (int q = threadIdx.x; q < (TY + 2) * (TX + 2); q += TY * TX) {
+            const int ly = q % (TY + 2), lx = q / (TY + 2);
+            const int gy = y0 + ly - 1, gx = x0 + lx - 1;
+            // adjoint massApply zeroes the Dirichlet ring before the convolution
+            const bool ok = gy > 0 && gx > 0 && gy < ny - 1 && gx < nx - 1;
+            L[lx][ly] = ok ? ls[(size_t)gy + (size_t)ny * gx] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        if (inside) {
+            double2 ml = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const float2 v = L[tx + b][ty + a];
+                    ml.x += w[a][b] * (double)v.x;
+                    ml.y += w[a][b] * (double)v.y;
+                }
+            const double2 av = zmul(scale[s], zmul(m, z_from(u[fs * s + idx])));
+            acc -= av.x * ml.x + av.y * ml.y;    // -Re(conj(av) * ml)
+        }
+        __syncthreads();
+    }
+    if (inside) grad[idx] += acc;
+}
+
+void gradient_launch(const float2 *u, const float2 *lam, const double2 *mult, const double2 *scale, int ny, int nx,
+                     int nb, double d, double e, double *grad, cudaStream_t st) {
+    dim3 grid(ceil_div(ny, TY), ceil_div(nx, TX));
+    gradient_kernel<<<grid, TY * TX, 0, st>>>(u, lam, mult, scale, ny, nx, nb, d, e, grad);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
+// out(:,:,s) = massApply(v(:,:,s) [.* mult .* dir], adjoint)
+template <bool CURV>
+__global__ void __launch_bounds__(TY * TX) mass_kernel(const float2 *v, const double2 *mult, const double *dir,
+                                                       float2 *out, int ny, int nx, int n, double d, double e,
+                                                       bool adjoint) {
+    __shared__ float2 V[TX + 2][TY + 2];
+    const int ty = threadIdx.x % TY, tx = threadIdx.x / TY;
+    const int y0 = blockIdx.x * TY, x0 = blockIdx.y * TX;
+    const int y = y0 + ty, x = x0 + tx;
+    const int s = blockIdx.z;
+    const size_t fs = (size_t)ny * nx * s;
+    for (int q = threadIdx.x; q < (TY + 2) * (TX + 2); q += TY * TX) {
+        const int ly = q % (TY + 2), lx = q / (TY + 2);
+        const int gy = y0 + ly - 1, gx = x0 + lx - 1;
+        float2 val = make_float2(0.f, 0.f);
+        if (gy >= 0 && gx >= 0 && gy < ny && gx < nx && !(adjoint && on_ring(gy, gx, ny, nx))) {
+            const size_t gi = (size_t)gy + (size_t)ny * gx;
+            if (CURV) {
+                const double2 w = zscale(dir[gi], zmul(mult[gi], z_from(v[fs + gi])));
+                val = c_from(w);
+            } else {
+                val = v[fs + gi];
+            }
+        }
+        V[lx][ly] = val;
+    }
+    __syncthreads();
+    if (y >= ny || x >= nx) return;
+    float2 acc = make_float2(0.f, 0.f);
+    if (adjoint || !on_ring(y, x, ny, nx)) {
+        const float c0 = (float)(1.0 - d - e), c1 = (float)(d / 4), c2 = (float)(e / 4);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const int k = (a != 1) + (b != 1);
+                const float wgt = k == 0 ? c0 : (k == 1 ? c1 : c2);
+                const float2 t = V[tx + b][ty + a];
+                acc.x = fmaf(wgt, t.x, acc.x);
+                acc.y = fmaf(wgt, t.y, acc.y);
+            }
+    }
+    out[fs + (size_t)y + (size_t)ny * x] = acc;
+}
+
+void mass_apply_launch(const float2 *v, float2 *out, int ny, int nx, int n, double d, double e, bool adjoint,
+                       cudaStream_t st) {
+    dim3 grid(ceil_div(ny, TY), ceil_div(nx, TX), n);
+    mass_kernel<false><<<grid, TY * TX, 0, st>>>(v, nullptr, nullptr, out, ny, nx, n, d, e, adjoint);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
+void curvature_source_launch(const float2 *u, const double2 *mult, const double *direction, float2 *out, int ny,
+                             int nx, int nb, double d, double e, cudaStream_t st) {
+    dim3 grid(ceil_div(ny, TY), ceil_div(nx, TX), nb);
+    mass_kernel<true><<<grid, TY * TX, 0, st>>>(u, mult, direction, out, ny, nx, nb, d, e, false);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
+__global__ void __launch_bounds__(FIT_THREADS) curvature_reduce_kernel(const float2 *u, const int32_t *rx_lin,
+                                                                       const uint8_t *mask, const double2 *scale,
+                                                                       int n_tx, int n_rx, int first_tx, int ny,
+                                                                       int nx, double *out) {
+    __shared__ double sh[FIT_THREADS / 32];
+    const int s = blockIdx.x, t = first_tx + s;
+    const float2 *us = u + (size_t)ny * nx * s;
+    double acc = 0;
+    for (int r = threadIdx.x; r < n_rx; r += FIT_THREADS) {
+        if (!mask[t + (size_t)n_tx * r]) continue;
+        const double2 v = zmul(z_from(us[rx_lin[r]]), scale[s]);
+        acc += zabs2(v);
+    }
+    acc = block_sum<FIT_THREADS>(acc, sh);
+    if (threadIdx.x == 0) out[s] = acc;
+}
+
+void curvature_reduce_launch(const float2 *u, const int32_t *rx_lin, const uint8_t *mask, const double2 *scale,
+                             int n_tx, int n_rx, int first_tx, int nb, int ny, int nx, double *out, cudaStream_t st) {
+    curvature_reduce_kernel<<<nb, FIT_THREADS, 0, st>>>(u, rx_lin, mask, scale, n_tx, n_rx, first_tx, ny, nx, out);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
+__global__ void virtual_source_kernel(const float2 *u, const double2 *mult, float2 *virt, size_t plane, size_t total) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+        virt[i] = c_from(zmul(mult[i % plane], z_from(u[i])));
+}
+
+void virtual_source_launch(const float2 *u, const double2 *mult, float2 *virt, int ny, int nx, int n, cudaStream_t st) {
+    const size_t plane = (size_t)ny * nx, total = plane * n;
+    const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    virtual_source_kernel<<<grid, 256, 0, st>>>(u, mult, virt, plane, total);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
+}  // namespace wust
