@@ -89,6 +89,26 @@ int wust_decomp_block_lu(const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 
                          const wust_c64 *Ud, const wust_c64 *Ul, const wust_c64 *Uu,
                          int Ny, int Nx, wust_c64 *invT, float *total_gpu_ms, void *stream);
 
+/* Largest Ny accepted by wust_decomp_block_lu_noalloc. */
+#define WUST_NOALLOC_MAX_NY 1024
+
+/* No counterpart in the reference (its MEX allocates through MATLAB).
+ * The same factorization as wust_decomp_block_lu, for callers that must not
+ * have the library allocate device memory: hosts whose own memory manager
+ * owns the device heap, and latency-critical callers that cannot afford the
+ * device synchronization of cudaMalloc/cudaFree.  It calls no cudaMalloc,
+ * cudaFree or allocating library routine; its ~8.9 MB of scratch is a static
+ * device array that every GPU loading the library holds until process exit.
+ * Ny must not exceed WUST_NOALLOC_MAX_NY (larger grids: WUST_ERR_INVALID_INPUT).
+ * All calls share that array, so calls that overlap on the GPU race; callers
+ * must serialize them.  The first call on each device looks up the array's
+ * address with that device current; make it before any stream capture.
+ * No timing output. */
+int wust_decomp_block_lu_noalloc(const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 *Lu,
+                                 const wust_c64 *Dd, const wust_c64 *Dl, const wust_c64 *Du,
+                                 const wust_c64 *Ud, const wust_c64 *Ul, const wust_c64 *Uu,
+                                 int Ny, int Nx, wust_c64 *invT, void *stream);
+
 /* Replaces `u = applyBlockLU(SRC,Ld,Ll,Lu,Ud,Ul,Uu,invT,adjoint)`
  * (Runtime/solver/applyBlockLU.cu:291-481; call site HelmholtzSolver.m:182-184).
  * src, u: Ny x Nx x n_src; u is caller-allocated and fully overwritten.

@@ -27,7 +27,7 @@ RETAIN_STATE = 2
 # Symbols that include/wust_b200.h declares (checked by the CPU tests).
 EXPORTED = (
     "wust_status_id", "wust_last_error", "wust_version",
-    "wust_decomp_block_lu", "wust_apply_block_lu",
+    "wust_decomp_block_lu", "wust_decomp_block_lu_noalloc", "wust_apply_block_lu",
     "wust_solver_create", "wust_solver_refactor", "wust_solver_destroy", "wust_solver_timings",
     "wust_solver_stencil", "wust_solver_block", "wust_solver_solve", "wust_solver_mass_apply",
     "wust_solver_oracle", "wust_solver_curvature", "wust_solver_stats",
@@ -75,6 +75,7 @@ def load() -> C.CDLL:
     lib.wust_last_error.argtypes = []
     lib.wust_version.argtypes = [pi, pi, pi]
     lib.wust_decomp_block_lu.argtypes = [vp] * 9 + [i, i, vp, C.POINTER(C.c_float), vp]
+    lib.wust_decomp_block_lu_noalloc.argtypes = [vp] * 9 + [i, i, vp, vp]
     lib.wust_apply_block_lu.argtypes = [vp, i, i, i] + [vp] * 7 + [i, vp, vp]
     lib.wust_solver_create.argtypes = [C.POINTER(vp), C.POINTER(SolverOptions), vp, vp, vp]
     lib.wust_solver_refactor.argtypes = [vp, vp, vp, d]

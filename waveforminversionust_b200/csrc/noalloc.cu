@@ -1,0 +1,106 @@
+// Allocation-free variant of the block-LU factorization entry point.
+//
+// Some callers cannot let a library call cudaMalloc/cudaFree: hosts whose own
+// GPU memory manager owns the device heap (MATLAB's gpuArray manager, caching
+// allocators of deep-learning frameworks) and may already have reserved most
+// of it, and latency-critical callers for which the implicit device
+// synchronization of cudaMalloc/cudaFree is not acceptable.  For them,
+// wust_decomp_block_lu_noalloc runs the same factorization kernel as
+// wust_decomp_block_lu, but its scratch (working page, row/column panels,
+// grid-barrier word and status words) lives in one file-scope __device__
+// array that is part of the loaded module: every GPU that loads the library
+// holds kNoallocScratchBytes for it until the process exits.
+//
+// Limits and sharing rules:
+//   * Ny <= WUST_NOALLOC_MAX_NY (1024); larger grids are rejected with
+//     WUST_ERR_INVALID_INPUT before any device work.
+//   * All calls on a device share the one array, which keeps whatever the
+//     last call left in it.  The launcher clears the barrier and status words
+//     at the start of every call; the working page and panels are fully
+//     rewritten before they are read.  Two calls whose work overlaps on the
+//     GPU (different streams, or host threads without ordering) race on the
+//     array and corrupt each other's results; callers must serialize them.
+//   * The first call on each device looks up the array's device address
+//     (cudaGetSymbolAddress) with that device current.  That lookup may load
+//     the module, so make the first call outside of any stream capture.
+#include <mutex>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace wust {
+
+constexpr int kNoallocMaxNy = WUST_NOALLOC_MAX_NY;
+// Scratch of factor_launch for Ny = kNoallocMaxNy, rounded up to 256 bytes.
+constexpr size_t kNoallocScratchBytes = ((size_t)(1024 * 1024 + 2 * 1024 * 32) * 8 + 1024 + 255) / 256 * 256;
+
+static __device__ __align__(256) unsigned char g_factor_scratch[kNoallocScratchBytes];
+
+static std::mutex g_noalloc_mutex;
+static void *g_noalloc_addr[64] = {};
+
+// Device address of g_factor_scratch on the current device (looked up once per device).
+static void *noalloc_scratch_address() {
+    int dev = 0;
+    WUST_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail(WUST_ERR_RUNTIME, "device ordinal %d out of range for the static scratch table", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *ptr = nullptr;
+        WUST_CUDA(cudaGetSymbolAddress(&ptr, g_factor_scratch));
+        if (!ptr) fail(WUST_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
+        g_noalloc_addr[dev] = ptr;
+    }
+    return g_noalloc_addr[dev];
+}
+
+static bool noalloc_device_pointer(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace wust
+
+using namespace wust;
+
+extern "C" int wust_decomp_block_lu_noalloc(const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 *Lu,
+                                            const wust_c64 *Dd, const wust_c64 *Dl, const wust_c64 *Du,
+                                            const wust_c64 *Ud, const wust_c64 *Ul, const wust_c64 *Uu, int Ny, int Nx,
+                                            wust_c64 *invT, void *stream) {
+    try {
+        if (Ny < 3 || Nx < 2 || (long long)Ny * Nx > 2147483647LL)
+            fail(WUST_ERR_INVALID_INPUT, "Block-LU grid must have an interior and fit int indexing.");
+        if (Ny > kNoallocMaxNy)
+            fail(WUST_ERR_INVALID_INPUT,
+                 "decompBlockLU without allocation supports Ny <= %d (got %d); use wust_decomp_block_lu", kNoallocMaxNy,
+                 Ny);
+        if (factor_scratch_bytes(Ny) > kNoallocScratchBytes)
+            fail(WUST_ERR_RUNTIME, "static scratch too small for Ny = %d", Ny);
+        const wust_c64 *in[9] = {Dd, Dl, Du, Ld, Ll, Lu, Ud, Ul, Uu};
+        for (const wust_c64 *p : in)
+            if (!p || !noalloc_device_pointer(p)) fail(WUST_ERR_INVALID_INPUT, "decompBlockLU requires 9 gpuArray inputs.");
+        if (!invT || !noalloc_device_pointer(invT))
+            fail(WUST_ERR_INVALID_OUTPUT, "decompBlockLU requires a device invT output.");
+        void *scratch = noalloc_scratch_address();
+        Coefs<float2> co;
+        co.Dd = (const float2 *)Dd; co.Dl = (const float2 *)Dl; co.Du = (const float2 *)Du;
+        co.Ld = (const float2 *)Ld; co.Ll = (const float2 *)Ll; co.Lu = (const float2 *)Lu;
+        co.Ud = (const float2 *)Ud; co.Ul = (const float2 *)Ul; co.Uu = (const float2 *)Uu;
+        co.ny = Ny; co.nx = Nx;
+        int hstat[3] = {0, 0, 0};
+        factor_launch(co, (float2 *)invT, scratch, kNoallocScratchBytes, (cudaStream_t)stream, 10.0, hstat);
+        if (hstat[2]) fail(WUST_ERR_DEVICE_TIMEOUT, "factorization grid barrier %d timed out", hstat[2]);
+        if (hstat[0]) fail(WUST_ERR_SINGULAR_SCHUR_BLOCK, "getrf block %d is singular at pivot %d", hstat[0], hstat[1] + 1);
+        return WUST_OK;
+    } catch (const WustError &e) {
+        set_last_error(e.message);
+        return e.status;
+    } catch (...) {
+        set_last_error("unknown error");
+        return WUST_ERR_RUNTIME;
+    }
+}
