@@ -34,9 +34,18 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-GRID = 552
-N_TX = 256
-FREQ = 1.2e6
+WORKLOADS = {
+    "config2": dict(n_tx=256, freq=1.2e6,
+                    text="config2 gradient: 552x552 grid (512^2 + 20-cell PML), dx 0.25 mm, 256 TX x 256 RX ring "
+                         "r = 55 mm, f = 1.2 MHz, breast-like phantom"),
+    # seconds-scale case used for ncu captures of the same kernels
+    "config1": dict(n_tx=32, freq=0.5e6,
+                    text="config1 gradient: 224x224 grid (192^2 + 16-cell PML), dx 0.4 mm, 32 TX x 128 RX ring "
+                         "r = 35 mm, f = 0.5 MHz, three elliptical inclusions"),
+}
+WORKLOAD = "config2"
+N_TX = WORKLOADS[WORKLOAD]["n_tx"]
+FREQ = WORKLOADS[WORKLOAD]["freq"]
 
 
 def flops_per_gradient(ny: int, nx: int, s: int) -> dict:
@@ -100,6 +109,8 @@ class ClockSampler:
 
 def make_problem(seed: int = 0):
     from waveforminversionust_b200 import synthetic
+    if WORKLOAD == "config1":
+        return synthetic.config1(seed=seed)
     return synthetic.config2(seed=seed, freqs=[FREQ])
 
 
@@ -146,8 +157,7 @@ def run_reference(args):
     line = dict(impl="reference", metric="gradients_per_second", value=v, unit="gradients/s", n_gpus=args.gpus,
                 steps=args.steps, warmup=args.warmup, ms_per_step=1e3 / v, higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="c128", data="synthetic",
-                config=dict(workload="config2 gradient: 552x552 grid (512^2 + 20-cell PML), dx 0.25 mm, 256 TX x "
-                                     "256 RX ring r = 55 mm, f = 1.2 MHz, breast-like phantom", global_batch=N_TX),
+                config=dict(workload=WORKLOADS[WORKLOAD]["text"], global_batch=N_TX),
                 cpu_baseline=dict(value=v, unit="gradients/s", cores=1, kind="port", sample=last["sample"]),
                 e2e=dict(value=v, unit="gradients/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
                 wall_seconds=wall)
@@ -182,7 +192,12 @@ def main():
     ap.add_argument("--precision", default="c64-refined")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="c64", help="extra precision profiles timed beside the headline")
+    ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
     args = ap.parse_args()
+    global WORKLOAD, N_TX, FREQ
+    WORKLOAD = args.workload
+    N_TX = WORKLOADS[WORKLOAD]["n_tx"]
+    FREQ = WORKLOADS[WORKLOAD]["freq"]
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -321,8 +336,7 @@ def main():
                 steps=args.steps, warmup=args.warmup, ms_per_step=head["ms_per_step"], higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype="c64+c128-refine" if args.precision != "c64" else "c64",
                 data="synthetic",
-                config=dict(workload="config2 gradient: 552x552 grid (512^2 + 20-cell PML), dx 0.25 mm, 256 TX x "
-                                     "256 RX ring r = 55 mm, f = 1.2 MHz, breast-like phantom",
+                config=dict(workload=WORKLOADS[WORKLOAD]["text"],
                             global_batch=N_TX * world, precision=args.precision, parallelism=f"replicas{world}",
                             l2="inputs larger than L2 (invT 1.35 GB, fields 0.62 GB)"),
                 e2e=head["e2e"], gpu_launches=int(round(head["launches_per_step"] * args.steps)),

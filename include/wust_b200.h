@@ -97,7 +97,7 @@ int wust_decomp_block_lu(const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 
  * have the library allocate device memory: hosts whose own memory manager
  * owns the device heap, and latency-critical callers that cannot afford the
  * device synchronization of cudaMalloc/cudaFree.  It calls no cudaMalloc,
- * cudaFree or allocating library routine; its ~8.9 MB of scratch is a static
+ * cudaFree or allocating library routine; its ~17.8 MB of scratch is a static
  * device array that every GPU loading the library holds until process exit.
  * Ny must not exceed WUST_NOALLOC_MAX_NY (larger grids: WUST_ERR_INVALID_INPUT).
  * All calls share that array, so calls that overlap on the GPU race; callers

@@ -8,6 +8,11 @@ namespace wust {
 enum SweepMode { SWEEP_F1 = 0, SWEEP_F2 = 1, SWEEP_A1 = 2, SWEEP_A2 = 3 };
 
 // ---- factor.cu -------------------------------------------------------------
+constexpr int kFactorTile = 48;
+// padded interior size of a working page (multiple of the output tile)
+constexpr size_t factor_pad(int ny) { return ((size_t)(ny - 2) + kFactorTile - 1) / kFactorTile * kFactorTile; }
+// two ping-pong working pages + barrier/status words
+constexpr size_t factor_scratch_bytes_for(int ny) { return 2 * factor_pad(ny) * factor_pad(ny) * 8 + 256; }
 size_t factor_scratch_bytes(int ny);
 // host_status (nullable, int[3]): {1+bad page, pivot, barrier timeout site};
 // when non-null the call synchronizes the stream.

@@ -32,7 +32,7 @@ namespace wust {
 
 constexpr int kNoallocMaxNy = WUST_NOALLOC_MAX_NY;
 // Scratch of factor_launch for Ny = kNoallocMaxNy, rounded up to 256 bytes.
-constexpr size_t kNoallocScratchBytes = ((size_t)(1024 * 1024 + 2 * 1024 * 32) * 8 + 1024 + 255) / 256 * 256;
+constexpr size_t kNoallocScratchBytes = (factor_scratch_bytes_for(kNoallocMaxNy) + 255) / 256 * 256;
 
 static __device__ __align__(256) unsigned char g_factor_scratch[kNoallocScratchBytes];
 
