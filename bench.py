@@ -183,6 +183,32 @@ def generate_observations(p, solver_cls, torch):
     return Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, [FREQ], Y, mask)
 
 
+def run_solves(args, p, solver_cls, torch):
+    """Factor once, then time forward solves of all transmitters (one line of JSON)."""
+    ny, nx = p.shape
+    s = solver_cls(p.x_m, p.y_m, p.c_init, None, FREQ, -1, 10.0, p.pml_m,
+                   dict(backend="gpu", stencil_bounds=(1400, 1700)), precision=args.precision, max_sources=N_TX)
+    src = torch.zeros((N_TX, nx, ny), dtype=torch.complex64, device="cuda")
+    lin = torch.as_tensor(p.tx_index - 1, device="cuda")
+    src.view(N_TX, -1)[torch.arange(N_TX, device="cuda"), lin] = 1
+    srcv = src.permute(2, 1, 0)
+    for _ in range(min(args.warmup, 1)):
+        s.solve(srcv)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        s.solve(srcv)
+    ev1.record()
+    torch.cuda.synchronize()
+    st = s.stats()
+    print(json.dumps(dict(mode="solve", precision=args.precision, workload=WORKLOADS[WORKLOAD]["text"],
+                          ms_per_solve=ev0.elapsed_time(ev1) / args.steps, factor_ms=s.factor_seconds * 1e3,
+                          refine_iters=st["refine_iters"], error_estimate=st["error_estimate"],
+                          final_residual=st["final_residual"], kernel_launches=st["kernel_launches"])), flush=True)
+    s.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -193,6 +219,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="c64", help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
+    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve"],
+                    help="solve: factor once, then time forward solves of all transmitters (kernel profiling)")
     args = ap.parse_args()
     global WORKLOAD, N_TX, FREQ
     WORKLOAD = args.workload
@@ -220,6 +248,9 @@ def main():
 
     p = make_problem(seed=rank)
     ny, nx = p.shape
+    if args.mode == "solve":
+        run_solves(args, p, HelmholtzSolver, torch)
+        return
     obs = generate_observations(p, HelmholtzSolver, torch)
     fl = flops_per_gradient(ny, nx, N_TX)
     stream = torch.cuda.current_stream()

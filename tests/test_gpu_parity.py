@@ -110,16 +110,25 @@ def test_solve_matches_sparse_lu(small):
     s.close()
 
 
-def test_refined_solve_reaches_fp64_accuracy(small):
+@pytest.mark.parametrize("precision", ["c64-refined", "tf32-refined"])
+def test_refined_solve_reaches_fp64_accuracy(small, precision):
     p, ref = small
     from oracle import helmholtz_fp64 as o
-    s = make_gpu_solver(p, p.c_true, p.frequencies_hz[0], precision="c64-refined")
+    s = make_gpu_solver(p, p.c_true, p.frequencies_hz[0], precision=precision)
     ny, nx = p.shape
     src = o.point_sources(p.tx_index, range(p.tx_index.size), ny, nx)
     u = to_np(s.solve(src.astype(np.complex64)))
     st = s.stats()
     assert st["refine_iters"] >= 1 and st["error_estimate"] <= 1e-5
     assert rel(u, ref.solve(src)) < 1e-5
+    # adjoint solve, interior (the block solver leaves the top/bottom border at zero)
+    rng = np.random.default_rng(4)
+    ny, nx = p.shape
+    r = np.zeros((ny, nx, 3), complex)
+    r[1:-1, 1:-1] = rng.standard_normal((ny - 2, nx - 2, 3)) + 1j * rng.standard_normal((ny - 2, nx - 2, 3))
+    lam = to_np(s.solve(r.astype(np.complex64), adjoint=True))
+    lam_ref = ref.solve(r, adjoint=True)
+    assert rel(lam[1:-1, 1:-1], lam_ref[1:-1, 1:-1]) < 1e-5
     s.close()
 
 
@@ -142,7 +151,8 @@ def _gpu_obs(o_obs):
                         o_obs.mask)
 
 
-@pytest.mark.parametrize("precision,tol_loss,tol_grad", [("c64", 1e-3, 1e-2), ("c64-refined", 1e-7, 1e-5)])
+@pytest.mark.parametrize("precision,tol_loss,tol_grad", [("c64", 1e-3, 1e-2), ("c64-refined", 1e-7, 1e-5),
+                                                        ("tf32-refined", 1e-7, 1e-5)])
 def test_oracle_matches_reference_fixture(ref_fixture, precision, tol_loss, tol_grad):
     """wust_oracle on the 31x31 fixture of test_runtime.m: loss and gradient."""
     from oracle import helmholtz_fp64 as o
@@ -228,7 +238,7 @@ def test_config1_gradient_parity():
     o_obs = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, p.frequencies_hz, Yobs, np.ones((32, 128, 1), bool))
     loss_ref, grad_ref, _ = o.wust_oracle(p.c_init, o_obs, 0, cfg_o)
     obs = Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, p.frequencies_hz, Yobs, np.ones((32, 128, 1), bool))
-    for precision, tl, tg in (("c64", 1e-3, 1e-2), ("c64-refined", 1e-6, 1e-4)):
+    for precision, tl, tg in (("c64", 1e-3, 1e-2), ("c64-refined", 1e-6, 1e-4), ("tf32-refined", 1e-6, 1e-4)):
         loss, grad = wust_oracle(p.c_init, obs, 0, default_config(pml_m=p.pml_m, precision=precision))
         assert abs(loss - loss_ref) / loss_ref < tl, precision
         assert rel(grad, grad_ref) < tg, precision

@@ -131,6 +131,10 @@ struct wust_solver {
     int ret_ntx = 0, ret_nrx = 0, ret_valid = 0;
     // host staging for pageable inputs
     double *stage_d = nullptr; size_t stage_d_cap = 0;
+    // tensor-core sweeps (TF32 profile): packed invT / invT^H operands, B operand, timeout flag
+    uint8_t *tc_afwd = nullptr, *tc_aadj = nullptr, *tc_b = nullptr;
+    int *tc_err = nullptr;
+    TcSweepGeom tc_geom{};
     float2 *stage_c = nullptr; size_t stage_c_cap = 0;
     double assembly_ms = 0, factor_ms = 0;
     int last_refine_iters = 0;
@@ -172,7 +176,7 @@ static void free_solver(wust_solver *s) {
     void *ptrs[] = {s->vel, s->atten, s->exi, s->eyi, s->mult, s->status, s->invT, s->fscratch, s->u, s->lam,
                     s->tmp, s->work, s->x64, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
                     s->rx_at, s->Yd, s->maskd, s->resid, s->scale, s->loss_src, s->grad, s->dir, s->ret_u,
-                    s->stage_d, s->stage_c};
+                    s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_err};
     for (void *p : ptrs) dfree(p);
     for (int i = 0; i < 9; ++i) { dfree(s->c128[i]); dfree(s->c64[i]); }
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
@@ -233,6 +237,8 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
     WUST_CUDA(cudaEventRecord(s->ev[1], st));
     int hstat[3] = {0, 0, 0};
     factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
+    if (s->precision == WUST_PRECISION_TF32_REFINED)
+        tc_pack_invT(s->invT, s->ny, s->nx, s->tc_geom, s->tc_afwd, s->tc_aadj, st);
     WUST_CUDA(cudaEventRecord(s->ev[2], st));
     int astat = 0;
     WUST_CUDA(cudaMemcpyAsync(&astat, s->status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -273,6 +279,28 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
     }
 }
 
+// One sweep pair (forward+backward) with the profile's arithmetic: CUDA-core
+// complex single, or tcgen05 TF32 GEMMs on the packed invT operands.
+static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
+    if (s->precision == WUST_PRECISION_TF32_REFINED) {
+        tc_sweep_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->tc_geom, src, S, adjoint, out, s->tmp, s->tc_b,
+                       s->tc_err, s->st);
+    } else {
+        sweep_solve(s->coefs64(), s->invT, src, S, adjoint, out, s->tmp, s->st);
+    }
+}
+
+static void check_tc_err(wust_solver *s) {
+    if (!s->tc_err) return;
+    int e = 0;
+    WUST_CUDA(cudaMemcpyAsync(&e, s->tc_err, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    WUST_CUDA(cudaStreamSynchronize(s->st));
+    if (e) {
+        WUST_CUDA(cudaMemsetAsync(s->tc_err, 0, sizeof(int), s->st));
+        fail(WUST_ERR_DEVICE_TIMEOUT, "tensor-core pipeline wait expired (code %d)", e);
+    }
+}
+
 // One block-LU solve with optional FP64 iterative refinement.  out must
 // differ from the dense source buffer.
 //
@@ -285,8 +313,7 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
 // the unrefined c64 solution while its error is not).
 static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
     cudaStream_t st = s->st;
-    const Coefs<float2> co = s->coefs64();
-    sweep_solve(co, s->invT, src, S, adjoint, out, s->tmp, st);
+    run_sweep(s, src, S, adjoint, out);
     s->last_refine_iters = 0;
     s->last_residual = -1;
     s->last_error_est = -1;
@@ -302,18 +329,20 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
     WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
     WUST_CUDA(cudaMemcpyAsync(bn.data(), s->bnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
     WUST_CUDA(cudaStreamSynchronize(st));
+    check_tc_err(s);
     for (int k = 1;; ++k) {
         if (k > s->refine_max)
             fail(WUST_ERR_NOT_CONVERGED, "refinement did not reach %.1e after %d correction solves (estimate %.3e)",
                  s->refine_tol, s->refine_max, s->last_error_est);
         rn_prev = rn;
-        sweep_solve(co, s->invT, dense, S, adjoint, s->d32, s->tmp, st);
+        run_sweep(s, dense, S, adjoint, s->d32);
         accumulate_launch(s->d32, s->x64, plane, S, s->dnorm2, s->xnorm2, st);
         residual_launch(s->coefs128(), src, s->x64, S, adjoint, s->r32, s->rnorm2, nullptr, st);
         WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaMemcpyAsync(dn.data(), s->dnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaMemcpyAsync(xn.data(), s->xnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaStreamSynchronize(st));
+        check_tc_err(s);
         double worst_err = 0, worst_res = 0;
         for (int q = 0; q < S; ++q) {
             if (!(std::isfinite(rn[q]) && std::isfinite(dn[q]) && std::isfinite(xn[q])))
@@ -455,8 +484,8 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         if (!(o->frequency_hz > 0) || !(o->pml_m > 0) || !std::isfinite(o->pml_strength))
             fail(WUST_ERR_INVALID_INPUT, "frequency, pml_m and pml_strength must be positive and finite");
         if (o->precision < 0 || o->precision > 3) fail(WUST_ERR_INVALID_INPUT, "unknown precision profile");
-        if (o->precision >= WUST_PRECISION_BF16_REFINED)
-            fail(WUST_ERR_INVALID_INPUT, "tensor-core precision profiles are not available in this build");
+        if (o->precision == WUST_PRECISION_BF16_REFINED)
+            fail(WUST_ERR_INVALID_INPUT, "the BF16 profile is not available in this build; use TF32");
         if (o->dispersion && !(o->time_step_s > 0 && o->reference_speed_mps > 0))
             fail(WUST_ERR_INVALID_INPUT, "LDR9 requires explicit simulation dispersion facts");
         s = new wust_solver();
@@ -519,6 +548,14 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
             s->bnorm2 = dalloc<double>(s->smax);
             s->dnorm2 = dalloc<double>(s->smax);
             s->xnorm2 = dalloc<double>(s->smax);
+        }
+        if (s->precision == WUST_PRECISION_TF32_REFINED) {
+            s->tc_geom = tc_sweep_geom(ny, s->smax);
+            s->tc_afwd = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
+            s->tc_aadj = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
+            s->tc_b = dalloc<uint8_t>(s->tc_geom.b_bytes);
+            s->tc_err = dalloc<int>(4);
+            WUST_CUDA(cudaMemset(s->tc_err, 0, 4 * sizeof(int)));
         }
         assemble_and_factor(s, vel, atten);
         *out = s;

@@ -25,6 +25,25 @@ int barrier_selftest(double timeout_s, int *site_out);
 void sweep_solve(const Coefs<float2> &co, const float2 *invT, const SrcView &src, int S, bool adjoint,
                  float2 *u, float2 *tmp, cudaStream_t st);
 
+// ---- tcsweep.cu (tensor-core sweeps, TF32 inputs) --------------------------
+struct TcSweepGeom {
+    int n;            // interior size ny - 2
+    int mt;           // 64-row complex tiles of the interior
+    int nk;           // interior rounded up to whole K chunks
+    int kc;           // K chunks of the stacked operand (2 nk / 32)
+    int nt;           // source tiles
+    size_t page_bytes;   // packed operand bytes per page
+    size_t b_bytes;      // packed B operand bytes
+};
+TcSweepGeom tc_sweep_geom(int ny, int S);
+// invT pages -> packed [Ar -Ai; Ai Ar] operands of invT_j and invT_j^H
+void tc_pack_invT(const float2 *invT, int ny, int nx, const TcSweepGeom &g, uint8_t *afwd, uint8_t *aadj,
+                  cudaStream_t st);
+// Same contract as sweep_solve; bt holds g.b_bytes, err receives a timeout flag.
+void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcSweepGeom &g,
+                    const SrcView &src, int S, bool adjoint, float2 *u, float2 *tmp, uint8_t *bt, int *err,
+                    cudaStream_t st);
+
 // ---- assemble.cu -----------------------------------------------------------
 struct AssemblyInput {
     int ny, nx;

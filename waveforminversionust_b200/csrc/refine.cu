@@ -11,83 +11,102 @@
 
 namespace wust {
 
-__device__ __forceinline__ double2 zfma_c(double2 acc, double2 a, double2 b, bool conj_a) {
-    if (conj_a) a.y = -a.y;
-    acc.x += a.x * b.x - a.y * b.y;
-    acc.y += a.x * b.y + a.y * b.x;
-    return acc;
-}
+constexpr int kResThreads = 128;
+constexpr int kResMaxS = 1024;          // per-block source norms kept in shared memory
 
+// One thread per grid point (y, x): its nine coefficients (or their
+// conjugates for H^H) are loaded once and reused for every source.
 template <bool ADJ>
-__global__ void residual_kernel(Coefs<double2> co, SrcView b, const double2 *x, int S, float2 *r32, double *rnorm2,
-                                double *bnorm2) {
+__global__ void __launch_bounds__(kResThreads) residual_kernel(Coefs<double2> co, SrcView b, const double2 *x, int S,
+                                                               float2 *r32, double *rnorm2, double *bnorm2) {
+    __shared__ double srr[kResMaxS], sbb[kResMaxS];
     const int ny = co.ny, nx = co.nx;
     const int y = blockIdx.x * blockDim.x + threadIdx.x;
     const int xi = blockIdx.y;
-    const int s = blockIdx.z;
-    double rr = 0, bb = 0;
-    if (y < ny && xi < nx) {
-        const size_t fs = (size_t)ny * nx * s;
-        const double2 *xs = x + fs;
-        auto X = [&](int yy, int xx) { return xs[(size_t)yy + (size_t)ny * xx]; };
-        double2 r = make_double2(0.0, 0.0);
-        if (y >= 1 && y <= ny - 2) {
-            double2 h = make_double2(0.0, 0.0);
-            if (!ADJ) {
-                h = zfma_c(h, co.dd(y, xi), X(y, xi), false);
-                h = zfma_c(h, co.dl(y - 1, xi), X(y - 1, xi), false);
-                h = zfma_c(h, co.du(y, xi), X(y + 1, xi), false);
-                if (xi >= 1) {
-                    h = zfma_c(h, co.ld(y, xi - 1), X(y, xi - 1), false);
-                    h = zfma_c(h, co.ll(y - 1, xi - 1), X(y - 1, xi - 1), false);
-                    h = zfma_c(h, co.lu(y, xi - 1), X(y + 1, xi - 1), false);
-                }
-                if (xi <= nx - 2) {
-                    h = zfma_c(h, co.ud(y, xi), X(y, xi + 1), false);
-                    h = zfma_c(h, co.ul(y - 1, xi), X(y - 1, xi + 1), false);
-                    h = zfma_c(h, co.uu(y, xi), X(y + 1, xi + 1), false);
-                }
-            } else {
-                h = zfma_c(h, co.dd(y, xi), X(y, xi), true);
-                h = zfma_c(h, co.dl(y, xi), X(y + 1, xi), true);
-                h = zfma_c(h, co.du(y - 1, xi), X(y - 1, xi), true);
-                if (xi <= nx - 2) {
-                    h = zfma_c(h, co.ld(y, xi), X(y, xi + 1), true);
-                    h = zfma_c(h, co.ll(y, xi), X(y + 1, xi + 1), true);
-                    h = zfma_c(h, co.lu(y - 1, xi), X(y - 1, xi + 1), true);
-                }
-                if (xi >= 1) {
-                    h = zfma_c(h, co.ud(y, xi - 1), X(y, xi - 1), true);
-                    h = zfma_c(h, co.ul(y, xi - 1), X(y + 1, xi - 1), true);
-                    h = zfma_c(h, co.uu(y - 1, xi - 1), X(y - 1, xi - 1), true);
-                }
-            }
-            const double2 bv = z_from(b.get(y, xi, s, ny, nx));
-            r = zsub(bv, h);
-            rr = zabs2(r);
-            bb = zabs2(bv);
+    for (int s = threadIdx.x; s < S; s += blockDim.x) { srr[s] = 0.0; sbb[s] = 0.0; }
+    __syncthreads();
+    const bool active = (y >= 1 && y <= ny - 2 && xi < nx);
+    // stencil taps: neighbour offsets (dy, dx) and coefficients
+    double2 w[9];
+    int dyv[9], dxv[9];
+    const double2 z = make_double2(0.0, 0.0);
+    if (active) {
+        const bool xl = xi >= 1, xr = xi <= nx - 2;
+        if (!ADJ) {
+            w[0] = co.dd(y, xi);               dyv[0] = 0;  dxv[0] = 0;
+            w[1] = co.dl(y - 1, xi);           dyv[1] = -1; dxv[1] = 0;
+            w[2] = co.du(y, xi);               dyv[2] = 1;  dxv[2] = 0;
+            w[3] = xl ? co.ld(y, xi - 1) : z;      dyv[3] = 0;  dxv[3] = -1;
+            w[4] = xl ? co.ll(y - 1, xi - 1) : z;  dyv[4] = -1; dxv[4] = -1;
+            w[5] = xl ? co.lu(y, xi - 1) : z;      dyv[5] = 1;  dxv[5] = -1;
+            w[6] = xr ? co.ud(y, xi) : z;          dyv[6] = 0;  dxv[6] = 1;
+            w[7] = xr ? co.ul(y - 1, xi) : z;      dyv[7] = -1; dxv[7] = 1;
+            w[8] = xr ? co.uu(y, xi) : z;          dyv[8] = 1;  dxv[8] = 1;
+        } else {
+            w[0] = zconj(co.dd(y, xi));            dyv[0] = 0;  dxv[0] = 0;
+            w[1] = zconj(co.dl(y, xi));            dyv[1] = 1;  dxv[1] = 0;
+            w[2] = zconj(co.du(y - 1, xi));        dyv[2] = -1; dxv[2] = 0;
+            w[3] = xr ? zconj(co.ld(y, xi)) : z;          dyv[3] = 0;  dxv[3] = 1;
+            w[4] = xr ? zconj(co.ll(y, xi)) : z;          dyv[4] = 1;  dxv[4] = 1;
+            w[5] = xr ? zconj(co.lu(y - 1, xi)) : z;      dyv[5] = -1; dxv[5] = 1;
+            w[6] = xl ? zconj(co.ud(y, xi - 1)) : z;      dyv[6] = 0;  dxv[6] = -1;
+            w[7] = xl ? zconj(co.ul(y, xi - 1)) : z;      dyv[7] = 1;  dxv[7] = -1;
+            w[8] = xl ? zconj(co.uu(y - 1, xi - 1)) : z;  dyv[8] = -1; dxv[8] = -1;
         }
-        r32[fs + (size_t)y + (size_t)ny * xi] = c_from(r);
-    }
-    // warp-level partial sums, one atomic per warp
+        // taps that leave the grid have zero weight; clamp their index
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        rr += __shfl_xor_sync(0xffffffffu, rr, o);
-        bb += __shfl_xor_sync(0xffffffffu, bb, o);
+        for (int t = 0; t < 9; ++t) {
+            const int xx = xi + dxv[t];
+            if (xx < 0 || xx >= nx) { dxv[t] = 0; w[t] = z; }
+        }
     }
-    if ((threadIdx.x & 31) == 0) {
-        if (rr != 0) atomicAdd(&rnorm2[s], rr);
-        if (bnorm2 && bb != 0) atomicAdd(&bnorm2[s], bb);
+    const size_t plane = (size_t)ny * nx;
+    const size_t me = (size_t)y + (size_t)ny * xi;
+    for (int s = 0; s < S; ++s) {
+        double rr = 0, bb = 0;
+        if (y < ny && xi < nx) {
+            double2 r = z;
+            if (active) {
+                const double2 *xs = x + plane * s;
+                double2 h = z;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) {
+                    const double2 v = xs[(size_t)(y + dyv[t]) + (size_t)ny * (xi + dxv[t])];
+                    h.x += w[t].x * v.x - w[t].y * v.y;
+                    h.y += w[t].x * v.y + w[t].y * v.x;
+                }
+                const double2 bv = z_from(b.get(y, xi, s, ny, nx));
+                r = zsub(bv, h);
+                rr = zabs2(r);
+                bb = zabs2(bv);
+            }
+            r32[plane * s + me] = c_from(r);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            rr += __shfl_xor_sync(0xffffffffu, rr, o);
+            bb += __shfl_xor_sync(0xffffffffu, bb, o);
+        }
+        if ((threadIdx.x & 31) == 0 && (rr != 0 || bb != 0)) {
+            atomicAdd(&srr[s], rr);
+            atomicAdd(&sbb[s], bb);
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        if (srr[s] != 0) atomicAdd(&rnorm2[s], srr[s]);
+        if (bnorm2 && sbb[s] != 0) atomicAdd(&bnorm2[s], sbb[s]);
     }
 }
 
 void residual_launch(const Coefs<double2> &co, const SrcView &b, const double2 *x, int S, bool adjoint, float2 *r32,
                      double *rnorm2, double *bnorm2, cudaStream_t st) {
+    if (S > kResMaxS) fail(WUST_ERR_INVALID_INPUT, "refined solves support at most %d sources per batch", kResMaxS);
     WUST_CUDA(cudaMemsetAsync(rnorm2, 0, sizeof(double) * S, st));
     if (bnorm2) WUST_CUDA(cudaMemsetAsync(bnorm2, 0, sizeof(double) * S, st));
-    dim3 grid(ceil_div(co.ny, 128), co.nx, S);
-    if (adjoint) residual_kernel<true><<<grid, 128, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
-    else residual_kernel<false><<<grid, 128, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
+    dim3 grid(ceil_div(co.ny, kResThreads), co.nx);
+    if (adjoint) residual_kernel<true><<<grid, kResThreads, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
+    else residual_kernel<false><<<grid, kResThreads, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
     ++g_kernel_launches;
     WUST_LAUNCH_CHECK();
 }

@@ -1,0 +1,197 @@
+// tcgen05 (5th-generation tensor core) building blocks for sm_100a.
+//
+// One CTA computes a 128 x TN fp32 tile D = A * B^T in tensor memory:
+//   A: 128 rows x K, B: TN rows x K, both K-major in the no-swizzle
+//      core-matrix layout (8 rows x 16 bytes per core matrix), stored in
+//      global memory already cut into K-chunks of 128 bytes per row, so one
+//      chunk of a tile is one contiguous block that a single cp.async.bulk
+//      moves into shared memory.
+//   Inside a chunk: core matrix (row group g, k group q) sits at
+//      g * 1024 + q * 128 bytes; rows of a core matrix are 16 bytes apart.
+//      -> leading byte offset (K direction) 128 B, stride byte offset
+//         (row-group direction) 1024 B.
+//   One MMA consumes 32 bytes of K (bf16: K = 16, tf32: K = 8), i.e. two
+//   core matrices, so the descriptor start advances 256 B per MMA.
+// The K loop runs through a STAGES-deep shared-memory ring: a single thread
+// issues the bulk copies (mbarrier complete_tx), the MMAs (accumulating in
+// TMEM) and tcgen05.commit arrivals that free a stage once its MMAs retired.
+// Every wait is bounded by a %globaltimer budget and reports failure.
+#pragma once
+
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace wust {
+namespace tc {
+
+constexpr int kChunkBytes = 128;                 // K bytes per row per chunk
+constexpr int kRowGroupBytes = 8 * kChunkBytes;  // 1024: one 8-row group of a chunk
+constexpr int kTileRows = 128;                   // MMA M
+constexpr int kAChunk = kTileRows * kChunkBytes; // 16 KB
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// Bounded parity wait: false when the budget ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase, unsigned long long timeout_ns) {
+    const uint32_t a = smem_u32(bar);
+    unsigned long long t0 = 0;
+    for (uint32_t spin = 0;; ++spin) {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (done) return true;
+        if ((spin & 63u) == 0) {
+            const unsigned long long t = global_timer_ns();
+            if (!t0) t0 = t;
+            else if (t - t0 > timeout_ns) return false;
+        }
+    }
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ uint64_t smem_desc(const void *p) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_u32(p) >> 4) & 0x3FFF);                 // start address
+    d |= (uint64_t)((kChunkBytes >> 4) & 0x3FFF) << 16;           // leading byte offset (K direction)
+    d |= (uint64_t)((kRowGroupBytes >> 4) & 0x3FFF) << 32;        // stride byte offset (row groups)
+    d |= (uint64_t)1 << 46;                                       // descriptor version for sm_100
+    return d;                                                     // base offset 0, no swizzle
+}
+// Instruction descriptor: D fp32, A/B tf32 (kind::tf32) or bf16 (kind::f16), both K-major.
+template <bool TF32>
+__host__ __device__ constexpr uint32_t instr_desc(int m, int n) {
+    return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(m >> 4) << 24);
+}
+
+template <bool TF32>
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+    if (TF32)
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p; }" ::"r"(
+                         tmem_d),
+                     "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+                     : "memory");
+    else
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p; }" ::"r"(
+                         tmem_d),
+                     "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+                     : "memory");
+}
+__device__ __forceinline__ void commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Warp-wide TMEM allocation (ncols: power of two >= 32); address lands in *slot.
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// 8 consecutive fp32 columns of this thread's TMEM lane (warp w reads lanes 32(w%4)..).
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+// Shared-memory footprint of a STAGES-deep ring for TN-row B tiles.
+template <int TN, int STAGES>
+struct Ring {
+    static constexpr int kBChunk = TN * kChunkBytes;
+    static constexpr int kBytes = STAGES * (kAChunk + kBChunk) + (2 * STAGES + 2) * 8 + 16;
+};
+
+// Single-thread K loop: D(tmem) = A * B^T over nchunks chunks.
+// A chunk c at a_base + c * a_stride, B chunk c at b_base + c * b_stride.
+// Returns false on a timed-out wait; always commits `done` at the end so the
+// epilogue can wait on it (phase = done_phase).
+template <bool TF32, int TN, int STAGES>
+__device__ bool tile_mainloop(uint8_t *sA, uint8_t *sB, uint64_t *full, uint64_t *empty, uint64_t *done,
+                              uint32_t (&full_phase)[STAGES], uint32_t (&empty_phase)[STAGES],
+                              const uint8_t *a_base, size_t a_stride, const uint8_t *b_base, size_t b_stride,
+                              int nchunks, uint32_t tmem, unsigned long long timeout_ns) {
+    constexpr int kB = TN * kChunkBytes;
+    constexpr uint32_t kIdesc = instr_desc<TF32>(kTileRows, TN);
+    bool ok = true;
+    int issued = 0;      // chunks whose copies were issued
+    int consumed = 0;    // chunks whose full barrier was waited
+    for (int c = 0; c < STAGES - 1 && c < nchunks; ++c) {
+        mbar_expect_tx(&full[c], kAChunk + kB);
+        bulk_g2s(sA + c * kAChunk, a_base + c * a_stride, kAChunk, &full[c]);
+        bulk_g2s(sB + c * kB, b_base + c * b_stride, kB, &full[c]);
+        ++issued;
+    }
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c % STAGES;
+        if (!mbar_wait(&full[s], full_phase[s], timeout_ns)) { ok = false; break; }
+        full_phase[s] ^= 1u;
+        ++consumed;
+        fence_after();
+#pragma unroll
+        for (int k = 0; k < kChunkBytes / 32; ++k)
+            mma<TF32>(tmem, smem_desc(sA + s * kAChunk + k * 256), smem_desc(sB + s * kB + k * 256), kIdesc,
+                      (c > 0 || k > 0) ? 1u : 0u);
+        commit(&empty[s]);
+        const int nc = c + STAGES - 1;
+        if (nc < nchunks) {
+            // stage nc % STAGES last held chunk c - 1: wait for its MMAs to retire
+            const int s2 = nc % STAGES;
+            if (c >= 1) {
+                if (!mbar_wait(&empty[s2], empty_phase[s2], timeout_ns)) { ok = false; break; }
+                empty_phase[s2] ^= 1u;
+            }
+            mbar_expect_tx(&full[s2], kAChunk + kB);
+            bulk_g2s(sA + s2 * kAChunk, a_base + nc * a_stride, kAChunk, &full[s2]);
+            bulk_g2s(sB + s2 * kB, b_base + nc * b_stride, kB, &full[s2]);
+            ++issued;
+        }
+    }
+    if (ok) {
+        // Chunks [max(0, nchunks - STAGES), nchunks) were committed but never
+        // waited; retire them so every stage's phase stays in step for the
+        // next tile that reuses the ring.
+        for (int c = (nchunks > STAGES ? nchunks - STAGES : 0); c < nchunks; ++c) {
+            const int s = c % STAGES;
+            if (!mbar_wait(&empty[s], empty_phase[s], timeout_ns)) { ok = false; break; }
+            empty_phase[s] ^= 1u;
+        }
+    } else {
+        // Let copies already in flight land before the CTA gives up (bounded).
+        for (int c = consumed; c < issued; ++c) {
+            const int s = c % STAGES;
+            if (mbar_wait(&full[s], full_phase[s], timeout_ns)) full_phase[s] ^= 1u;
+        }
+    }
+    commit(done);
+    return ok;
+}
+
+}  // namespace tc
+}  // namespace wust
