@@ -132,6 +132,37 @@ def test_refined_solve_reaches_fp64_accuracy(small, precision):
     s.close()
 
 
+def test_tensor_core_sweep_split_k_and_source_batches():
+    """TF32 tensor-core sweeps on a grid whose K range is split over 4 CTAs,
+    with a partial source tile and more sources than one launch holds, agree
+    with the complex-single sweeps once both are refined in FP64."""
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    ny = nx = 330
+    dx = 0.3e-3
+    x = (np.arange(nx) - (nx - 1) / 2) * dx
+    y = (np.arange(ny) - (ny - 1) / 2) * dx
+    X, Y = np.meshgrid(x, y)
+    c = 1500 + 40 * np.exp(-((X - 5e-3) ** 2 + Y ** 2) / (2 * (12e-3) ** 2))
+    sols = {}
+    for precision in ("c64-refined", "tf32-refined"):
+        s = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, 16 * dx, dict(backend="gpu", stencil_bounds=(1400, 1700)),
+                            precision=precision, refine_tol=1e-9, max_sources=400)
+        out = {}
+        for adjoint, S in ((False, 400), (True, 150)):
+            r = np.zeros((ny, nx, S), np.complex64)
+            g = np.random.default_rng(11 + S)
+            r[1:-1, 1:-1] = (g.standard_normal((ny - 2, nx - 2, S)) + 1j * g.standard_normal((ny - 2, nx - 2, S)))
+            out[adjoint] = to_np(s.solve(r, adjoint=adjoint))
+            st = s.stats()
+            assert st["error_estimate"] <= 1e-9, (precision, adjoint, st)
+        sols[precision] = out
+        s.close()
+    for adjoint in (False, True):
+        a = sols["tf32-refined"][adjoint][1:-1, 1:-1]
+        b = sols["c64-refined"][adjoint][1:-1, 1:-1]
+        assert rel(a, b) < 1e-7, adjoint
+
+
 def test_mass_apply_matches_oracle(small):
     p, ref = small
     s = make_gpu_solver(p, p.c_true, p.frequencies_hz[0])

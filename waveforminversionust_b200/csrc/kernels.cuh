@@ -29,20 +29,27 @@ void sweep_solve(const Coefs<float2> &co, const float2 *invT, const SrcView &src
 struct TcSweepGeom {
     int n;            // interior size ny - 2
     int mt;           // 64-row complex tiles of the interior
-    int nk;           // interior rounded up to whole K chunks
-    int kc;           // K chunks of the stacked operand (2 nk / 32)
-    int nt;           // source tiles
-    size_t page_bytes;   // packed operand bytes per page
-    size_t b_bytes;      // packed B operand bytes
+    int kc;           // K chunks: 16 complex interior rows (32 interleaved re/im values) each
+    int ks;           // K split: CTAs sharing one output tile
+    int per;          // K chunks per CTA
+    int nt;           // 64-source tiles per launch (source batch = 64 nt)
+    size_t page_bytes;    // packed operand bytes per page
+    size_t part_bytes;    // split-K partial tiles of one launch
+    size_t tmp_elems;     // complex elements of the adjoint double buffer
+    int sync_words;       // group + tile counters
 };
-TcSweepGeom tc_sweep_geom(int ny, int S);
+// max_ctas: CTAs that can be co-resident (cooperative launch, one per SM).
+TcSweepGeom tc_sweep_geom(int ny, int S, int max_ctas);
+int tc_sweep_max_ctas();
 // invT pages -> packed [Ar -Ai; Ai Ar] operands of invT_j and invT_j^H
 void tc_pack_invT(const float2 *invT, int ny, int nx, const TcSweepGeom &g, uint8_t *afwd, uint8_t *aadj,
                   cudaStream_t st);
-// Same contract as sweep_solve; bt holds g.b_bytes, err receives a timeout flag.
+// Same contract as sweep_solve: u (ny*nx*S) is overwritten.  Scratch:
+// tmp (g.tmp_elems), part (g.part_bytes), sync (g.sync_words); err receives
+// the site of an expired device wait.
 void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcSweepGeom &g,
-                    const SrcView &src, int S, bool adjoint, float2 *u, float2 *tmp, uint8_t *bt, int *err,
-                    cudaStream_t st);
+                    const SrcView &src, int S, bool adjoint, float2 *u, float2 *tmp, float *part, unsigned *sync,
+                    int *err, cudaStream_t st);
 
 // ---- assemble.cu -----------------------------------------------------------
 struct AssemblyInput {
