@@ -131,10 +131,9 @@ struct wust_solver {
     int ret_ntx = 0, ret_nrx = 0, ret_valid = 0;
     // host staging for pageable inputs
     double *stage_d = nullptr; size_t stage_d_cap = 0;
-    // tensor-core sweeps (TF32 profile): packed invT / invT^H operands, adjoint
-    // double buffer, split-K partial tiles, barrier counters, wait-site flag
-    uint8_t *tc_afwd = nullptr, *tc_aadj = nullptr;
-    float2 *tc_tmp = nullptr;
+    // tensor-core sweeps (TF32 profile): packed invT / invT^H operands, packed
+    // B chunks, split-K partial tiles, barrier counters, wait-site flag
+    uint8_t *tc_afwd = nullptr, *tc_aadj = nullptr, *tc_b = nullptr;
     float *tc_part = nullptr;
     unsigned *tc_sync = nullptr;
     int *tc_err = nullptr;
@@ -180,7 +179,7 @@ static void free_solver(wust_solver *s) {
     void *ptrs[] = {s->vel, s->atten, s->exi, s->eyi, s->mult, s->status, s->invT, s->fscratch, s->u, s->lam,
                     s->tmp, s->work, s->x64, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
                     s->rx_at, s->Yd, s->maskd, s->resid, s->scale, s->loss_src, s->grad, s->dir, s->ret_u,
-                    s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_tmp, s->tc_part, s->tc_sync, s->tc_err};
+                    s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err};
     for (void *p : ptrs) dfree(p);
     for (int i = 0; i < 9; ++i) { dfree(s->c128[i]); dfree(s->c64[i]); }
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
@@ -287,7 +286,7 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
 // complex single, or tcgen05 TF32 GEMMs on the packed invT operands.
 static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
     if (s->precision == WUST_PRECISION_TF32_REFINED) {
-        tc_sweep_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->tc_geom, src, S, adjoint, out, s->tc_tmp,
+        tc_sweep_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->tc_geom, src, S, adjoint, out, s->tc_b,
                        s->tc_part, s->tc_sync, s->tc_err, s->st);
     } else {
         sweep_solve(s->coefs64(), s->invT, src, S, adjoint, out, s->tmp, s->st);
@@ -557,7 +556,7 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
             s->tc_geom = tc_sweep_geom(ny, s->smax, tc_sweep_max_ctas());
             s->tc_afwd = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
             s->tc_aadj = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
-            s->tc_tmp = dalloc<float2>(s->tc_geom.tmp_elems);
+            s->tc_b = dalloc<uint8_t>(s->tc_geom.b_bytes);
             s->tc_part = dalloc<float>(s->tc_geom.part_bytes / sizeof(float));
             s->tc_sync = dalloc<unsigned>(s->tc_geom.sync_words);
             s->tc_err = dalloc<int>(4);

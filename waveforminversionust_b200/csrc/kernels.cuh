@@ -35,8 +35,8 @@ struct TcSweepGeom {
     int nt;           // 64-source tiles per launch (source batch = 64 nt)
     size_t page_bytes;    // packed operand bytes per page
     size_t part_bytes;    // split-K partial tiles of one launch
-    size_t tmp_elems;     // complex elements of the adjoint double buffer
-    int sync_words;       // group + tile counters
+    size_t b_bytes;       // packed B chunks of one launch
+    int sync_words;       // group counters
 };
 // max_ctas: CTAs that can be co-resident (cooperative launch, one per SM).
 TcSweepGeom tc_sweep_geom(int ny, int S, int max_ctas);
@@ -45,10 +45,10 @@ int tc_sweep_max_ctas();
 void tc_pack_invT(const float2 *invT, int ny, int nx, const TcSweepGeom &g, uint8_t *afwd, uint8_t *aadj,
                   cudaStream_t st);
 // Same contract as sweep_solve: u (ny*nx*S) is overwritten.  Scratch:
-// tmp (g.tmp_elems), part (g.part_bytes), sync (g.sync_words); err receives
+// bglob (g.b_bytes), part (g.part_bytes), sync (g.sync_words); err receives
 // the site of an expired device wait.
 void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcSweepGeom &g,
-                    const SrcView &src, int S, bool adjoint, float2 *u, float2 *tmp, float *part, unsigned *sync,
+                    const SrcView &src, int S, bool adjoint, float2 *u, uint8_t *bglob, float *part, unsigned *sync,
                     int *err, cudaStream_t st);
 
 // ---- assemble.cu -----------------------------------------------------------

@@ -17,22 +17,25 @@
 // Work split: output tiles of 64 complex rows x 64 sources; the K range of a
 // tile is split over `ks` <= 4 CTAs (at most 9 K chunks of 16 complex rows
 // each, so every CTA keeps its whole A slice and B slice in shared memory).
-// The split-K partial tiles go through L2 and each CTA of the tile sums one
-// column slice in rank order (deterministic).  Grid = (M tiles, source tiles,
-// ks), one CTA per SM, launched cooperatively; tiles of different sources
-// never wait on each other.
+// Grid = (M tiles, source tiles, ks), one CTA per SM, launched cooperatively;
+// the CTAs of one source tile form a group that synchronises through one
+// monotonic counter, and groups of different sources never wait on each other.
 //
 // Per step and CTA (8 warps):
-//   stage B: every load the step depends on is issued at once (the previous
-//     column, the base term, two edge rows), then the stencil is evaluated
-//     with weights staged in shared memory and written straight into the MMA
-//     operand layout;
-//   one thread issues the MMAs; the next step's A chunks are copied
-//     (cp.async.bulk) as soon as they retire, so the HBM stream of invT
-//     overlaps the epilogue and the barriers;
-//   partial tile -> L2, next step's weights -> shared memory, tile barrier,
-//   reduce one column slice, write the column, group barrier.
-// Every wait is bounded and reports its site through *err.
+//   bulk-copy this step's packed B chunks (produced once per chunk, below)
+//     into shared memory; one thread issues the MMAs; the next step's A
+//     chunks are copied (cp.async.bulk) as soon as they retire, so the HBM
+//     stream of invT overlaps the epilogue and the barriers;
+//   TMEM -> split-K partial tile in L2; prefetch the next step's static
+//     inputs; group barrier;
+//   each CTA owns whole K chunks (16 rows) of the next B: it sums the split-K
+//     partials of those rows plus a 2-row halo (fixed rank order, so results
+//     are deterministic), finishes column j of u for them, evaluates the
+//     stencil of the next step and writes the packed chunk to L2; group
+//     barrier.
+// So every B value is computed once, and the only data exchanged per step
+// is the partial tiles and the packed B chunks.  Every wait is bounded and
+// reports its site through *err.
 #include <algorithm>
 
 #include "common.cuh"
@@ -45,15 +48,13 @@ constexpr int TN = 64;                       // sources per tile (MMA N)
 constexpr int kRowsPerChunk = 16;            // complex rows per K chunk (32 fp32 K values)
 constexpr int kMaxPer = 9;                   // K chunks per CTA
 constexpr int kMaxKSplit = 4;
-constexpr int kMaxRows = kMaxPer * kRowsPerChunk;   // 144 complex rows per CTA
-constexpr int kQuads = kMaxRows / 4;                // 36 row quads
 constexpr int kSweepThreads = 256;
+constexpr int kMaxOwned = 3;                        // B chunks produced per CTA and step
 constexpr int kBChunk = TN * tc::kChunkBytes;       // 8 KB
 constexpr size_t kSmemA = (size_t)kMaxPer * tc::kAChunk;
 constexpr size_t kSmemB = (size_t)kMaxPer * kBChunk;
 constexpr size_t kSmemBar = 256;
-constexpr size_t kSmemW = 3 * kMaxRows * sizeof(float2);
-constexpr size_t kSweepSmem = kSmemA + kSmemB + kSmemBar + kSmemW;
+constexpr size_t kSweepSmem = kSmemA + kSmemB + kSmemBar;
 static_assert(kSweepSmem <= 232448, "shared memory of one CTA");
 
 // byte offset of element (row, ke) inside one chunk of a 128-row (or TN-row) tile
@@ -82,6 +83,10 @@ TcSweepGeom tc_sweep_geom(int ny, int S, int max_ctas) {
     if (g.ks > kMaxKSplit)
         fail(WUST_ERR_INVALID_INPUT, "tensor-core sweep supports Ny <= %d (got %d)",
              kMaxKSplit * kMaxPer * kRowsPerChunk + 2, ny);
+    // every CTA of a source tile produces at most kMaxOwned B chunks per step
+    while (g.kc > kMaxOwned * g.mt * g.ks && g.ks < kMaxKSplit) g.ks *= 2;
+    if (g.kc > kMaxOwned * g.mt * g.ks)
+        fail(WUST_ERR_INVALID_INPUT, "tensor-core sweep: grid shape Ny = %d not supported", ny);
     g.per = ceil_div(g.kc, g.ks);
     const int per_tile = g.mt * g.ks;
     if (per_tile > max_ctas)
@@ -90,8 +95,8 @@ TcSweepGeom tc_sweep_geom(int ny, int S, int max_ctas) {
     g.nt = std::max(1, std::min(ceil_div(std::max(S, 1), TN), max_ctas / per_tile));
     g.page_bytes = (size_t)g.mt * g.kc * tc::kAChunk;
     g.part_bytes = (size_t)g.mt * g.nt * g.ks * 128 * TN * sizeof(float);
-    g.tmp_elems = 2 * (size_t)ny * g.nt * TN;
-    g.sync_words = g.nt + g.mt * g.nt;
+    g.b_bytes = (size_t)g.nt * g.kc * kBChunk;
+    g.sync_words = g.nt;
     return g;
 }
 
@@ -152,18 +157,17 @@ struct SweepParams {
     Coefs<float2> co;
     SrcView src;
     float2 *u;                // [ny, nx, S] (global source index)
-    float2 *tmp;              // adjoint: two [ny, tb] buffers (launch-local source index)
+    uint8_t *bglob;           // packed B chunks of the next step: [nt][kc] x kBChunk
     float *part;              // [tile][ks][128][TN]
     unsigned *group_ctr;      // [nt]
-    unsigned *tile_ctr;       // [mt * nt]
     int *err;
     int ny, nx, n, mt, kc, ks, per;
-    int s0, s_end, tb;        // global sources [s0, s_end) of this launch; tmp row pitch tb
+    int s0, s_end;            // global sources [s0, s_end) of this launch
     unsigned long long timeout_ns;
 };
 
 // Device-wait sites reported through *err.
-enum { SITE_COPY = 1, SITE_MMA = 2, SITE_TILE = 3, SITE_GROUP = 4 };
+enum { SITE_COPY = 1, SITE_MMA = 2, SITE_GROUP = 4, SITE_B = 5 };
 
 // Optional phase timer (SM cycles of CTA (0,0,0), summed over steps), built
 // only into profiling builds of the library.
@@ -192,12 +196,14 @@ __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y
 
 // Arrive on a monotonic counter and wait until it reaches target (bounded).
 // __syncthreads on both sides; the result is uniform over the CTA and false
-// when this or another CTA gave up.
+// when this or another CTA gave up.  Global writes made before the call are
+// visible to the other CTAs' generic and async-proxy (bulk copy) reads after it.
 __device__ __forceinline__ bool counter_sync(unsigned *ctr, unsigned target, int *err, int *s_ok,
                                              unsigned long long timeout_ns, int site) {
     __syncthreads();
     if (threadIdx.x == 0) {
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        asm volatile("fence.proxy.async.global;" ::: "memory");
         asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(ctr), "r"(1u) : "memory");
         int ok = 1;
         const unsigned long long t0 = global_timer_ns();
@@ -214,6 +220,7 @@ __device__ __forceinline__ bool counter_sync(unsigned *ctr, unsigned target, int
                 }
             }
         }
+        asm volatile("fence.proxy.async.global;" ::: "memory");
         *s_ok = ok;
     }
     __syncthreads();
@@ -226,185 +233,55 @@ __device__ __forceinline__ int step_col(int i, int nx, bool &fwd) {
     return fwd ? 1 + i : (nx - 2) - (i - (nx - 1));
 }
 
-// Stencil weights of step (fwd, j) for this CTA's rows, so that
-//     B(y) = base(y) - (wc(y) c(y) + wm(y) c(y-1) + wp(y) c(y+1)),
-// c = the column the step depends on:
-//   !ADJ fwd: L_{j-1} of u(:, j-1)     base = SRC_j
-//   !ADJ bwd: -U_j of u(:, j+1)         base = 0
-//   ADJ fwd:  U_{j-2}^H of tmp          base = SRC_{j-1}   (j == 1: B = u(:, 0))
-//   ADJ bwd:  L_j^H of u(:, j+1)        base = u(:, j)
+// B of step (fwd, j) at grid row y:  B(y) = base(y) - (wc c(y) + wm c(y-1) + wp c(y+1)),
+// c = the column the step depends on (the previous step's GEMM result):
+//   !ADJ fwd: c = u(:, j-1), L_{j-1}            base = SRC_j
+//   !ADJ bwd: c = u(:, j+1), -U_j               base = 0
+//   ADJ fwd:  c = tmp_{j-1}, U_{j-2}^H          base = SRC_{j-1}   (j == 1: B = u(:, 0) = 0)
+//   ADJ bwd:  c = u(:, j+1), L_j^H              base = u(:, j)
+// (applyBlockLU.cu:433-467; the ADJ forward value B is also u(:, j-1)).
+// Weights that would reach outside the grid are zero.
 template <bool ADJ>
-__device__ __forceinline__ void stage_weights(const SweepParams &p, float2 *w, int y0, int rows, bool fwd, int j) {
-    const Coefs<float2> &co = p.co;
-    for (int r = threadIdx.x; r < rows; r += kSweepThreads) {
-        const int yp = y0 + r, y = yp + 1;
-        float2 wc = f2(0.f, 0.f), wm = wc, wp = wc;
-        if (yp < p.n) {
-            if (!ADJ && fwd) {
-                wc = co.ld(y, j - 1); wm = co.ll(y - 1, j - 1); wp = co.lu(y, j - 1);
-            } else if (!ADJ) {
-                wc = co.ud(y, j); wm = co.ul(y - 1, j); wp = co.uu(y, j);
-                wc = f2(-wc.x, -wc.y); wm = f2(-wm.x, -wm.y); wp = f2(-wp.x, -wp.y);
-            } else if (fwd) {
-                if (j >= 2) {
-                    wc = cconj(co.ud(y, j - 2)); wm = cconj(co.uu(y - 1, j - 2)); wp = cconj(co.ul(y, j - 2));
-                } else {
-                    wc = f2(-1.f, 0.f);
-                }
-            } else {
-                wc = cconj(co.ld(y, j)); wm = cconj(co.lu(y - 1, j)); wp = cconj(co.ll(y, j));
-            }
-        }
-        w[r] = wc;
-        w[kMaxRows + r] = wm;
-        w[2 * kMaxRows + r] = wp;
-    }
-}
-
-// Registers of one thread's share of a B slice: the column values c and the
-// base term of its 36 items, and the two window-edge rows.
-struct StageRegs {
-    float2 c[kQuads], base[kQuads];
-    float2 e_lo, e_hi;
-};
-
-// Issue every load of this CTA's B slice of step (fwd, j).  Warp w owns
-// sources 8w..8w+7; lane = (source & 7, row & 3), item q = row quad, so each
-// source reads 32 contiguous bytes of a column per item.
-template <bool ADJ>
-__device__ __forceinline__ void stage_b_load(const SweepParams &p, StageRegs &R, int nt, int c0, int nch, bool fwd,
-                                             int j) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s8 = lane & 7, r4 = lane >> 3;
-    const int ny = p.ny, nx = p.nx;
-    const size_t plane = (size_t)ny * nx;
-    const int y0 = kRowsPerChunk * c0;
-    const int nq = 4 * nch;
-    const int sl = 8 * warp + s8;                   // source within the tile
-    const int sb = nt * TN + sl;                    // source within the launch
-    const int s = p.s0 + sb;                        // global source
-    const bool sv = s < p.s_end;
-    const bool from_tmp = ADJ && (fwd ? j >= 2 : j <= nx - 3);
-    const int fcol = fwd ? (ADJ ? 0 : j - 1) : (ADJ ? nx - 1 : j + 1);
-    const float2 *tbuf = p.tmp + (size_t)ny * p.tb * (fwd ? ((j - 1) & 1) : ((j + 1) & 1));
-    const float2 *col = from_tmp ? tbuf + (size_t)ny * sb : p.u + plane * s + (size_t)ny * fcol;
-    // base term: SRC column bx, u(:, j) (ADJ bwd) or zero
-    const int bx = (!ADJ && fwd) ? j : ((ADJ && fwd && j >= 2) ? j - 1 : -1);
-    const float2 *ubase = (ADJ && !fwd) ? p.u + plane * s + (size_t)ny * j : nullptr;
-    float2 *c = R.c, *base = R.base;
-#pragma unroll
-    for (int q = 0; q < kQuads; ++q) {
-        c[q] = f2(0.f, 0.f);
-        base[q] = f2(0.f, 0.f);
-        if (q < nq && sv) {
-            const int yp = y0 + 4 * q + r4, y = yp + 1;
-            if (yp <= p.n) c[q] = __ldcg(col + y);
-            if (yp < p.n) {
-                if (ubase) {
-                    base[q] = __ldcg(ubase + y);
-                } else if (bx >= 0) {
-                    if (p.src.mode == SRC_DENSE) {
-                        base[q] = p.src.dense[(size_t)y + (size_t)ny * bx + plane * s];
-                    } else if (p.src.mode == SRC_POINT) {
-                        base[q] = (p.src.lin[s] == y + ny * bx) ? f2(1.f, 0.f) : f2(0.f, 0.f);
-                    } else if (p.src.mode == SRC_SCATTER) {
-                        const int k = p.src.at[(size_t)y + (size_t)ny * bx];
-                        base[q] = k >= 0 ? p.src.vals[k + (size_t)p.src.n_slots * s] : f2(0.f, 0.f);
-                    }
-                }
-            }
-        }
-    }
-    R.e_lo = f2(0.f, 0.f);
-    R.e_hi = f2(0.f, 0.f);
-    if (sv && r4 == 0) R.e_lo = __ldcg(col + y0);                       // row before the window
-    const int yhi = y0 + kRowsPerChunk * nch + 1;                      // row after the window
-    if (sv && r4 == 3 && yhi <= ny - 1) R.e_hi = __ldcg(col + yhi);
-}
-
-// Evaluate the stencil and write the B slice into shared memory, in the
-// operand layout: element (source sl, complex row yp) of chunk (yp - y0)/16
-// at chunk_off(sl, 2 * ((yp - y0) % 16)); the 8-byte stores of a warp cover
-// all 32 banks.  The stencil neighbours come from the lane 8 apart in the
-// same quad or the lane 24 apart in the neighbouring quad (one shuffle
-// each), the two window edges from R.  ADJ modes also write the finished
-// column of the previous step into u (write_u: the CTAs of M tile 0 own that).
-template <bool ADJ>
-__device__ __forceinline__ void stage_b_compute(const SweepParams &p, const StageRegs &R, uint8_t *sB,
-                                                const float2 *w, int nt, int c0, int nch, bool fwd, int j,
-                                                bool write_u) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s8 = lane & 7, r4 = lane >> 3;
-    const int ny = p.ny, nx = p.nx;
-    const size_t plane = (size_t)ny * nx;
-    const int y0 = kRowsPerChunk * c0;
-    const int nq = 4 * nch;
-    const int sl = 8 * warp + s8;
-    const int sb = nt * TN + sl;
-    const int s = p.s0 + sb;
-    const bool sv = s < p.s_end;
-    const float2 *tbuf = p.tmp + (size_t)ny * p.tb * (fwd ? ((j - 1) & 1) : ((j + 1) & 1));
-    const float2 *c = R.c, *base = R.base;
-
-    float2 *ucol = nullptr;   // column of u finished by the previous step (ADJ)
-    if (ADJ && write_u && sv) {
-        if (fwd && j >= 2) ucol = p.u + plane * s + (size_t)ny * (j - 1);
-        if (!fwd && j <= nx - 3) ucol = p.u + plane * s + (size_t)ny * (j + 1);
-    }
-    const int lane_m = (r4 == 0) ? lane + 24 : lane - 8;
-    const int lane_p = (r4 == 3) ? lane - 24 : lane + 8;
-#pragma unroll
-    for (int q = 0; q < kQuads; ++q) {
-        if (q < nq) {
-            const float2 sup_m = (r4 == 3 && q > 0) ? c[q > 0 ? q - 1 : 0] : c[q];
-            const float2 sup_p = (r4 == 0 && q + 1 < kQuads) ? c[q + 1 < kQuads ? q + 1 : q] : c[q];
-            float2 m, pn;
-            m.x = __shfl_sync(0xffffffffu, sup_m.x, lane_m);
-            m.y = __shfl_sync(0xffffffffu, sup_m.y, lane_m);
-            pn.x = __shfl_sync(0xffffffffu, sup_p.x, lane_p);
-            pn.y = __shfl_sync(0xffffffffu, sup_p.y, lane_p);
-            if (q == 0 && r4 == 0) m = R.e_lo;
-            if (q == nq - 1 && r4 == 3) pn = R.e_hi;
-            const int r = 4 * q + r4;                 // row within the window
-            const int yp = y0 + r;
-            float2 b = f2(0.f, 0.f);
-            if (sv && yp < p.n) {
-                float2 acc = cmul(w[r], c[q]);
-                cfma(acc, w[kMaxRows + r], m);
-                cfma(acc, w[2 * kMaxRows + r], pn);
-                b = csub(base[q], acc);
-                if (ucol) ucol[yp + 1] = (fwd ? b : c[q]);
-            }
-            *reinterpret_cast<float2 *>(sB + (q >> 2) * kBChunk + chunk_off(sl, 2 * (4 * (q & 3) + r4))) =
-                f2(to_tf32(b.x), to_tf32(b.y));
-        }
-    }
-    // border rows of the finished column (ADJ): rows 0 / ny-1 computed in the
-    // forward sweep, zero in the backward sweep
-    if (ADJ && ucol && r4 == 0) {
-        const Coefs<float2> &co = p.co;
-        const bool first = (c0 == 0);
-        const bool last = (y0 <= p.n - 1) && (y0 + kRowsPerChunk * nch >= p.n);
-        if (fwd) {
-            const float2 *t = tbuf + (size_t)ny * sb;
-            if (first) {
-                float2 acc = f2(0.f, 0.f);
-                cfma_conj(acc, co.ud(0, j - 2), __ldcg(t));
-                cfma_conj(acc, co.ul(0, j - 2), __ldcg(t + 1));
-                ucol[0] = csub(p.src.get(0, j - 1, s, ny, nx), acc);
-            }
-            if (last) {
-                float2 acc = f2(0.f, 0.f);
-                cfma_conj(acc, co.ud(ny - 1, j - 2), __ldcg(t + ny - 1));
-                cfma_conj(acc, co.uu(ny - 2, j - 2), __ldcg(t + ny - 2));
-                ucol[ny - 1] = csub(p.src.get(ny - 1, j - 1, s, ny, nx), acc);
-            }
+__device__ __forceinline__ void step_weights(const Coefs<float2> &co, bool fwd, int j, int y, float2 &wc, float2 &wm,
+                                             float2 &wp) {
+    const int ny = co.ny;
+    const float2 z = f2(0.f, 0.f);
+    wc = z; wm = z; wp = z;
+    if (!ADJ && fwd) {
+        wc = co.ld(y, j - 1); wm = co.ll(y - 1, j - 1); wp = co.lu(y, j - 1);
+    } else if (!ADJ) {
+        const float2 a = co.ud(y, j), b = co.ul(y - 1, j), c = co.uu(y, j);
+        wc = f2(-a.x, -a.y); wm = f2(-b.x, -b.y); wp = f2(-c.x, -c.y);
+    } else if (fwd) {
+        if (j >= 2) {
+            wc = cconj(co.ud(y, j - 2));
+            if (y > 0) wm = cconj(co.uu(y - 1, j - 2));
+            if (y < ny - 1) wp = cconj(co.ul(y, j - 2));
         } else {
-            if (first) ucol[0] = f2(0.f, 0.f);
-            if (last) ucol[ny - 1] = f2(0.f, 0.f);
+            wc = f2(-1.f, 0.f);
         }
+    } else {
+        wc = cconj(co.ld(y, j)); wm = cconj(co.lu(y - 1, j)); wp = cconj(co.ll(y, j));
     }
 }
+template <bool ADJ>
+__device__ __forceinline__ float2 step_base(const SweepParams &p, bool fwd, int j, int y, int s) {
+    if (!ADJ && fwd) return p.src.get(y, j, s, p.ny, p.nx);
+    if (!ADJ) return f2(0.f, 0.f);
+    if (fwd) return j >= 2 ? p.src.get(y, j - 1, s, p.ny, p.nx) : f2(0.f, 0.f);
+    return __ldcg(p.u + (size_t)p.ny * p.nx * s + (size_t)p.ny * j + y);
+}
+
+// Shared-memory scratch of the reduce/produce phase (inside the B stage area,
+// which is free between the MMAs and the next step's B copy).
+constexpr int kHalo = 2;
+constexpr int kCRows = kRowsPerChunk + 2 * kHalo;          // 20
+constexpr size_t kOffC = 0;                                 // c: [kCRows][TN] float2
+constexpr size_t kOffC2 = kOffC + (size_t)kCRows * TN * 8;  // transformed c (ADJ fwd -> bwd turn)
+constexpr size_t kOffStage = kOffC2 + (size_t)kCRows * TN * 8;
+constexpr size_t kOffPre = kOffStage + kBChunk;             // prefetch: [kMaxOwned][kCRows][TN] float2
+constexpr size_t kOffW = kOffPre + (size_t)kMaxOwned * kCRows * TN * 8;   // weights: [kMaxOwned][3][16] float2
+static_assert(kOffW + (size_t)kMaxOwned * 3 * kRowsPerChunk * 8 <= kSmemB, "reduce scratch fits the B stage area");
 
 template <bool ADJ, int KS>
 __global__ void __launch_bounds__(kSweepThreads, 1) tc_sweep_kernel(SweepParams p) {
@@ -415,22 +292,27 @@ __global__ void __launch_bounds__(kSweepThreads, 1) tc_sweep_kernel(SweepParams 
     uint64_t *done = full + kMaxPer;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     int *s_ok = reinterpret_cast<int *>(tmem_slot + 1);
-    float2 *sW = reinterpret_cast<float2 *>(smem + kSmemA + kSmemB + kSmemBar);
+    float2 *cbuf = reinterpret_cast<float2 *>(sB + kOffC);
+    float2 *cbuf2 = reinterpret_cast<float2 *>(sB + kOffC2);
+    uint8_t *stage = sB + kOffStage;
+    float2 *pre = reinterpret_cast<float2 *>(sB + kOffPre);
+    float2 *wbuf = reinterpret_cast<float2 *>(sB + kOffW);
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const int mt = blockIdx.x, nt = blockIdx.y, ks = blockIdx.z;
-    const int ny = p.ny, nx = p.nx;
+    const int ny = p.ny, nx = p.nx, n = p.n;
     const size_t plane = (size_t)ny * nx;
     const int c0 = ks * p.per;
     const int nch = max(0, min(p.kc, c0 + p.per) - c0);
-    const int y0 = kRowsPerChunk * c0;
     const int tile = mt + p.mt * nt;
-    const unsigned group_size = (unsigned)(p.mt * KS);
-    const int rank_in_group = mt + p.mt * ks;
+    const int G = p.mt * KS;                       // CTAs of this source tile
+    const int rank = mt + p.mt * ks;               // this CTA's rank among them
     const int nsteps = 2 * (nx - 1);
+    uint8_t *bg = p.bglob + (size_t)nt * p.kc * kBChunk;
+    const int sbase = p.s0 + nt * TN;              // global index of source 0 of this tile
 
     if (tid == 0) {
-        for (int q = 0; q < kMaxPer; ++q) tc::mbar_init(&full[q], 1);
+        for (int q = 0; q < kMaxPer; ++q) tc::mbar_init(&full[q], 2);   // A copy + B copy of chunk q
         tc::mbar_init(done, 1);
         tc::mbar_fence_init();
     }
@@ -452,15 +334,88 @@ __global__ void __launch_bounds__(kSweepThreads, 1) tc_sweep_kernel(SweepParams 
         }
     };
 
+    // Produce the packed B chunk Q of step (fwd1, j1) from c (rows 16Q-2 ..
+    // 16Q+17 at cbuf rows 0..19) and the prefetched base (pre_k rows 0..15);
+    // ADJ forward steps also write B into u(:, j1-1) (with its border rows).
+    auto produce = [&](int Q, const float2 *c, const float2 *pre_k, const float2 *w_k, bool fwd1, int j1) {
+        const int s_l = tid & (TN - 1);
+        const int s = sbase + s_l;
+        const bool sv = s < p.s_end;
+        for (int yl = tid >> 6; yl < kRowsPerChunk; yl += kSweepThreads / TN) {
+            const int yp = kRowsPerChunk * Q + yl, y = yp + 1;
+            float2 b = f2(0.f, 0.f);
+            if (sv && yp < n) {
+                const int r = yl + kHalo;
+                float2 acc = cmul(w_k[yl], c[r * TN + s_l]);
+                cfma(acc, w_k[kRowsPerChunk + yl], c[(r - 1) * TN + s_l]);
+                cfma(acc, w_k[2 * kRowsPerChunk + yl], c[(r + 1) * TN + s_l]);
+                b = csub(pre_k[yl * TN + s_l], acc);
+                if (ADJ && fwd1) p.u[plane * s + (size_t)ny * (j1 - 1) + y] = b;
+            }
+            *reinterpret_cast<float2 *>(stage + chunk_off(s_l, 2 * yl)) = f2(to_tf32(b.x), to_tf32(b.y));
+        }
+        if (ADJ && fwd1 && sv && tid < TN) {
+            // border rows 0 and ny-1 of u(:, j1-1) (no B entry)
+            for (int e = 0; e < 2; ++e) {
+                const int yp = e == 0 ? -1 : n;
+                const int r = yp - kRowsPerChunk * Q + kHalo;
+                if (r < 1 || r > kCRows - 2) continue;
+                const int y = yp + 1;
+                float2 wc, wm, wp;
+                step_weights<ADJ>(p.co, fwd1, j1, y, wc, wm, wp);
+                float2 acc = cmul(wc, c[r * TN + s_l]);
+                cfma(acc, wm, c[(r - 1) * TN + s_l]);
+                cfma(acc, wp, c[(r + 1) * TN + s_l]);
+                p.u[plane * s + (size_t)ny * (j1 - 1) + y] = csub(step_base<ADJ>(p, fwd1, j1, y, s), acc);
+            }
+        }
+        __syncthreads();
+        const float4 *src4 = reinterpret_cast<const float4 *>(stage);
+        float4 *dst4 = reinterpret_cast<float4 *>(bg + (size_t)Q * kBChunk);
+        for (int v = tid; v < kBChunk / 16; v += kSweepThreads) dst4[v] = src4[v];
+        __syncthreads();
+    };
+
+    // Prefetch (static data of the next step, or the old column that a
+    // subtracting step needs) for owned chunk Q into pre_k.
+    auto prefetch = [&](int Q, float2 *pre_k, float2 *w_k, bool fwd1, int j1, bool old_of_j, int j) {
+        constexpr int kItems = kCRows * TN / kSweepThreads;   // 5: all loads in flight before any store
+        float2 v[kItems];
+#pragma unroll
+        for (int m = 0; m < kItems; ++m) {
+            const int idx = tid + kSweepThreads * m;
+            const int s_l = idx / kCRows, r = idx % kCRows;    // consecutive rows per source
+            const int s = sbase + s_l;
+            v[m] = f2(0.f, 0.f);
+            if (s < p.s_end) {
+                if (old_of_j) {
+                    const int yp = kRowsPerChunk * Q - kHalo + r;
+                    if (yp >= 0 && yp < n) v[m] = __ldcg(p.u + plane * s + (size_t)ny * j + yp + 1);
+                } else if (r < kRowsPerChunk) {
+                    const int yp = kRowsPerChunk * Q + r;
+                    if (yp < n) v[m] = step_base<ADJ>(p, fwd1, j1, yp + 1, s);
+                }
+            }
+        }
+        if (tid < kRowsPerChunk) {
+            const int yp = kRowsPerChunk * Q + tid;
+            float2 wc = f2(0.f, 0.f), wm = wc, wp = wc;
+            if (yp < n) step_weights<ADJ>(p.co, fwd1, j1, yp + 1, wc, wm, wp);
+            w_k[tid] = wc;
+            w_k[kRowsPerChunk + tid] = wm;
+            w_k[2 * kRowsPerChunk + tid] = wp;
+        }
+#pragma unroll
+        for (int m = 0; m < kItems; ++m) {
+            const int idx = tid + kSweepThreads * m;
+            pre_k[(idx % kCRows) * TN + idx / kCRows] = v[m];
+        }
+    };
+
     int a_step = -1;          // step whose A copies are in flight (thread 0)
     if (tid == 0 && nch > 0) {
         issue_a(0);
         a_step = 0;
-    }
-    {
-        bool f0;
-        const int j0 = step_col(0, nx, f0);
-        stage_weights<ADJ>(p, sW, y0, kRowsPerChunk * nch, f0, j0);
     }
     unsigned group_epoch = 0;
     bool ok = true;
@@ -468,56 +423,31 @@ __global__ void __launch_bounds__(kSweepThreads, 1) tc_sweep_kernel(SweepParams 
     long long prof_t = clock64();
 #endif
 
-    for (int i = 0; i < nsteps; ++i) {
+    // prologue: B of step 0 from c = 0
+    {
+        bool f0;
+        const int j0 = step_col(0, nx, f0);
+        for (int k = 0, Q = rank; Q < p.kc; ++k, Q += G) {
+            for (int idx = tid; idx < kCRows * TN; idx += kSweepThreads) cbuf[idx] = f2(0.f, 0.f);
+            prefetch(Q, pre, wbuf, f0, j0, false, 0);
+            __syncthreads();
+            produce(Q, cbuf, pre, wbuf, f0, j0);
+        }
+        group_epoch += (unsigned)G;
+        ok = counter_sync(p.group_ctr + nt, group_epoch, p.err, s_ok, p.timeout_ns, SITE_B);
+    }
+
+    for (int i = 0; i < nsteps && ok; ++i) {
         bool fwd;
         const int j = step_col(i, nx, fwd);
-
-        if (ADJ && i == nx - 1) {
-            // u(:, nx-1) = SRC_{nx-1} - U_{nx-2}^H tmp  (every row)
-            const float2 *t0 = p.tmp + (size_t)ny * p.tb * ((nx - 1) & 1);
-            for (int idx = rank_in_group * kSweepThreads + tid; idx < ny * TN;
-                 idx += (int)group_size * kSweepThreads) {
-                const int y = idx % ny, sl = idx / ny;
-                const int sb = nt * TN + sl, s = p.s0 + sb;
-                if (s >= p.s_end) continue;
-                const float2 *t = t0 + (size_t)ny * sb;
-                float2 acc = f2(0.f, 0.f);
-                cfma_conj(acc, p.co.ud(y, nx - 2), __ldcg(t + y));
-                if (y > 0) cfma_conj(acc, p.co.uu(y - 1, nx - 2), __ldcg(t + y - 1));
-                if (y < ny - 1) cfma_conj(acc, p.co.ul(y, nx - 2), __ldcg(t + y + 1));
-                p.u[plane * s + (size_t)ny * (nx - 1) + y] = csub(p.src.get(y, nx - 1, s, ny, nx), acc);
-            }
-            group_epoch += group_size;
-            if (!counter_sync(p.group_ctr + nt, group_epoch, p.err, s_ok, p.timeout_ns, SITE_GROUP)) {
-                ok = false;
-                break;
-            }
-        }
-
-        // ---- B operand ------------------------------------------------------
         SPROF(0);
-        {
-            StageRegs R;
-            stage_b_load<ADJ>(p, R, nt, c0, nch, fwd, j);
-#ifdef WUST_SWEEP_PROFILE
-            {   // wait for every load (profiling builds only)
-                float d = R.e_lo.x + R.e_hi.x;
-#pragma unroll
-                for (int q = 0; q < kQuads; ++q) d += R.c[q].x + R.base[q].y;
-                if (d == 1.2345e30f) sW[0] = f2(d, d);
-                SPROF(9);
-            }
-#endif
-            stage_b_compute<ADJ>(p, R, sB, sW, nt, c0, nch, fwd, j, mt == 0);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc::fence_before();
-        __syncthreads();
-        tc::fence_after();
-        SPROF(1);
 
-        // ---- MMAs (one thread) -----------------------------------------------
+        // ---- B of this step -> shared memory; MMAs (one thread) -------------
         if (tid == 0) {
+            for (int q = 0; q < nch; ++q) {
+                tc::mbar_expect_tx(&full[q], kBChunk);
+                tc::bulk_g2s(sB + (size_t)q * kBChunk, bg + (size_t)(c0 + q) * kBChunk, kBChunk, &full[q]);
+            }
             constexpr uint32_t kIdesc = tc::instr_desc<true>(tc::kTileRows, TN);
             int got = 0;
             for (int q = 0; q < nch; ++q) {
@@ -537,10 +467,9 @@ __global__ void __launch_bounds__(kSweepThreads, 1) tc_sweep_kernel(SweepParams 
             a_step = -1;
             tc::commit(done);
         }
-        SPROF(7);
+        SPROF(1);
         if (!tc::mbar_wait(done, (uint32_t)(i & 1), p.timeout_ns)) atomicCAS(p.err, 0, SITE_MMA);
         tc::fence_after();
-        SPROF(8);
         if (tid == 0) *s_ok = (*(volatile int *)p.err == 0);
         __syncthreads();
         if (!*s_ok) {
@@ -571,99 +500,126 @@ __global__ void __launch_bounds__(kSweepThreads, 1) tc_sweep_kernel(SweepParams 
                 __stcg(reinterpret_cast<float4 *>(mypart + cb + 4), make_float4(t[4], t[5], t[6], t[7]));
             }
         }
-        // weights of the next step (the stencil of this step is done)
-        if (i + 1 < nsteps) {
-            bool f1;
-            const int j1 = step_col(i + 1, nx, f1);
-            stage_weights<ADJ>(p, sW, y0, kRowsPerChunk * nch, f1, j1);
+        tc::fence_before();
+        // static inputs of the next step (or the old column of a subtracting
+        // step) for the owned chunks, read before anyone rewrites column j
+        bool fwd1 = false;
+        int j1 = 0;
+        const bool has_next = i + 1 < nsteps;
+        if (has_next) j1 = step_col(i + 1, nx, fwd1);
+        const bool sub = !ADJ && !fwd;
+        for (int k = 0, Q = rank; Q < p.kc; ++k, Q += G) {
+            float2 *pre_k = pre + (size_t)k * kCRows * TN;
+            float2 *w_k = wbuf + (size_t)k * 3 * kRowsPerChunk;
+            if (sub) prefetch(Q, pre_k, w_k, fwd1, j1, true, j);
+            else if (has_next) prefetch(Q, pre_k, w_k, fwd1, j1, false, j);
         }
         SPROF(3);
-        tc::fence_before();
-        if (KS > 1) {
-            if (!counter_sync(p.tile_ctr + tile, (unsigned)(KS * (i + 1)), p.err, s_ok, p.timeout_ns, SITE_TILE)) {
-                ok = false;
-                break;
-            }
-        } else {
-            __syncthreads();
-        }
-        tc::fence_after();
-        SPROF(4);
-
-        // ---- reduce one column slice over the KS partials, write the column ---
-        {
-            constexpr int CPR = TN / KS, QTR = CPR / 4, NV = QTR / 4;   // columns per thread, float4 per rank
-            const int ir = tid & 63, qt = tid >> 6;
-            const int cb = ks * CPR + qt * QTR;
-            const float *pt = p.part + (size_t)tile * KS * 128 * TN;
-            float4 re[KS][NV], im[KS][NV];
-#pragma unroll
-            for (int r = 0; r < KS; ++r)
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    re[r][v] = __ldcg(reinterpret_cast<const float4 *>(pt + ((size_t)r * 128 + ir) * TN + cb + 4 * v));
-                    im[r][v] =
-                        __ldcg(reinterpret_cast<const float4 *>(pt + ((size_t)r * 128 + ir + 64) * TN + cb + 4 * v));
-                }
-            const int gi = mt * 64 + ir;
-            if (gi < p.n) {
-                float2 old[NV][4];
-                if (!ADJ && !fwd) {
-#pragma unroll
-                    for (int v = 0; v < NV; ++v)
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const int s = p.s0 + nt * TN + cb + 4 * v + q;
-                            old[v][q] =
-                                s < p.s_end ? __ldcg(p.u + plane * s + (size_t)ny * j + gi + 1) : f2(0.f, 0.f);
-                        }
-                }
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    float4 sr = re[0][v], si = im[0][v];
-#pragma unroll
-                    for (int r = 1; r < KS; ++r) {
-                        sr.x += re[r][v].x; sr.y += re[r][v].y; sr.z += re[r][v].z; sr.w += re[r][v].w;
-                        si.x += im[r][v].x; si.y += im[r][v].y; si.z += im[r][v].z; si.w += im[r][v].w;
-                    }
-                    const float vr[4] = {sr.x, sr.y, sr.z, sr.w}, vi[4] = {si.x, si.y, si.z, si.w};
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int sb = nt * TN + cb + 4 * v + q;
-                        const int s = p.s0 + sb;
-                        if (s >= p.s_end) continue;
-                        if (ADJ) {
-                            p.tmp[(size_t)ny * p.tb * (j & 1) + (size_t)ny * sb + gi + 1] = f2(vr[q], vi[q]);
-                        } else {
-                            float2 *dst = p.u + plane * s + (size_t)ny * j + gi + 1;
-                            *dst = fwd ? f2(vr[q], vi[q]) : f2(old[v][q].x - vr[q], old[v][q].y - vi[q]);
-                        }
-                    }
-                }
-            }
-        }
-        SPROF(5);
-        group_epoch += group_size;
+        group_epoch += (unsigned)G;
         if (!counter_sync(p.group_ctr + nt, group_epoch, p.err, s_ok, p.timeout_ns, SITE_GROUP)) {
             ok = false;
             break;
         }
+        tc::fence_after();
+        SPROF(4);
+
+        // ---- owned chunks: reduce the K split, finish column j, produce B ------
+        for (int k = 0, Q = rank; Q < p.kc; ++k, Q += G) {
+            float2 *pre_k = pre + (size_t)k * kCRows * TN;
+            {
+                const int s_l = tid & (TN - 1);
+#pragma unroll
+                for (int rr = 0; rr < kCRows / 4; ++rr) {
+                    const int r = (tid >> 6) + 4 * rr;
+                    const int yp = kRowsPerChunk * Q - kHalo + r;
+                    float2 v = f2(0.f, 0.f);
+                    if (yp >= 0 && yp < n) {
+                        const int t2 = yp / 64 + p.mt * nt, rw = yp % 64;
+                        const float *pt = p.part + (size_t)t2 * KS * 128 * TN + (size_t)rw * TN + s_l;
+                        float re[KS], im[KS];
+#pragma unroll
+                        for (int q = 0; q < KS; ++q) {
+                            re[q] = __ldcg(pt + (size_t)q * 128 * TN);
+                            im[q] = __ldcg(pt + (size_t)q * 128 * TN + 64 * TN);
+                        }
+#pragma unroll
+                        for (int q = 0; q < KS; ++q) { v.x += re[q]; v.y += im[q]; }
+                        if (sub) {
+                            const float2 o = pre_k[r * TN + s_l];
+                            v = f2(o.x - v.x, o.y - v.y);
+                        }
+                    }
+                    cbuf[r * TN + s_l] = v;
+                }
+            }
+            __syncthreads();
+            const float2 *c = cbuf;
+            if (ADJ && fwd && j == nx - 1) {
+                // turn of the H^H solve: w = u(:, nx-1) = SRC_{nx-1} - U_{nx-2}^H t, every row
+                for (int idx = tid; idx < kCRows * TN; idx += kSweepThreads) {
+                    const int r = idx / TN, s_l = idx % TN;
+                    const int yp = kRowsPerChunk * Q - kHalo + r, y = yp + 1;
+                    const int s = sbase + s_l;
+                    float2 w = f2(0.f, 0.f);
+                    if (r >= 1 && r <= kCRows - 2 && y >= 0 && y <= ny - 1 && s < p.s_end) {
+                        float2 acc = f2(0.f, 0.f);
+                        cfma_conj(acc, p.co.ud(y, nx - 2), cbuf[r * TN + s_l]);
+                        if (y > 0) cfma_conj(acc, p.co.uu(y - 1, nx - 2), cbuf[(r - 1) * TN + s_l]);
+                        if (y < ny - 1) cfma_conj(acc, p.co.ul(y, nx - 2), cbuf[(r + 1) * TN + s_l]);
+                        w = csub(p.src.get(y, nx - 1, s, ny, nx), acc);
+                        const bool own = (yp >= kRowsPerChunk * Q && yp < kRowsPerChunk * (Q + 1) && yp < n) ||
+                                         (yp == -1) || (yp == n);
+                        if (own) p.u[plane * s + (size_t)ny * (nx - 1) + y] = w;
+                    }
+                    cbuf2[idx] = w;
+                }
+                __syncthreads();
+                c = cbuf2;
+            }
+            // finished column j of u (own rows; ADJ backward: zero border rows)
+            if (!ADJ || !fwd) {
+                for (int idx = tid; idx < kRowsPerChunk * TN; idx += kSweepThreads) {
+                    const int s_l = idx / kRowsPerChunk, yl = idx % kRowsPerChunk;
+                    const int yp = kRowsPerChunk * Q + yl;
+                    const int s = sbase + s_l;
+                    if (yp < n && s < p.s_end) p.u[plane * s + (size_t)ny * j + yp + 1] = c[(yl + kHalo) * TN + s_l];
+                }
+                if (ADJ && tid < TN && sbase + tid < p.s_end) {
+                    const int s = sbase + tid;
+                    if (Q == 0) p.u[plane * s + (size_t)ny * j] = f2(0.f, 0.f);
+                    if (Q == p.kc - 1) p.u[plane * s + (size_t)ny * j + ny - 1] = f2(0.f, 0.f);
+                }
+            }
+            if (has_next) {
+                if (sub) {
+                    // the subtracting step's prefetch held the old column; the
+                    // next step (also backward) has base 0
+                    for (int idx = tid; idx < kCRows * TN; idx += kSweepThreads) pre_k[idx] = f2(0.f, 0.f);
+                    __syncthreads();
+                }
+                produce(Q, c, pre_k, wbuf + (size_t)k * 3 * kRowsPerChunk, fwd1, j1);
+            } else {
+                __syncthreads();
+            }
+        }
+        SPROF(5);
+        if (has_next) {
+            group_epoch += (unsigned)G;
+            if (!counter_sync(p.group_ctr + nt, group_epoch, p.err, s_ok, p.timeout_ns, SITE_B)) {
+                ok = false;
+                break;
+            }
+        }
         SPROF(6);
     }
 
-    if (ADJ && ok) {
-        // u(:, 0) = [0; tmp; 0] from the last backward step (j = 0)
-        const float2 *t0 = p.tmp;
-        for (int idx = rank_in_group * kSweepThreads + tid; idx < ny * TN; idx += (int)group_size * kSweepThreads) {
-            const int y = idx % ny, sl = idx / ny;
-            const int sb = nt * TN + sl, s = p.s0 + sb;
-            if (s >= p.s_end) continue;
-            p.u[plane * s + y] = (y == 0 || y == ny - 1) ? f2(0.f, 0.f) : __ldcg(t0 + (size_t)ny * sb + y);
-        }
-    }
-    // copies still in flight after a failure: let them land (bounded)
+    // A copies still in flight after a failure: stand in for the B arrival
+    // that will not come, then let them land (bounded)
     if (tid == 0 && a_step >= 0)
-        for (int q = 0; q < nch; ++q) tc::mbar_wait(&full[q], (uint32_t)(a_step & 1), p.timeout_ns);
+        for (int q = 0; q < nch; ++q) {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&full[q])) : "memory");
+            tc::mbar_wait(&full[q], (uint32_t)(a_step & 1), p.timeout_ns);
+        }
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
@@ -714,7 +670,7 @@ static void launch_sweep(const SweepParams &p, dim3 grid, cudaStream_t st) {
 }
 
 void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcSweepGeom &g,
-                    const SrcView &src, int S, bool adjoint, float2 *u, float2 *tmp, float *part, unsigned *sync,
+                    const SrcView &src, int S, bool adjoint, float2 *u, uint8_t *bglob, float *part, unsigned *sync,
                     int *err, cudaStream_t st) {
     configure_all();
     const int ny = co.ny, nx = co.nx;
@@ -726,7 +682,7 @@ void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t 
     p.co = co;
     p.src = src;
     p.u = u;
-    p.tmp = tmp;
+    p.bglob = bglob;
     p.part = part;
     p.err = err;
     p.ny = ny;
@@ -736,17 +692,14 @@ void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t 
     p.kc = g.kc;
     p.ks = g.ks;
     p.per = g.per;
-    p.tb = g.nt * TN;
     p.timeout_ns = 1000000000ull;
     for (int s0 = 0; s0 < S; s0 += g.nt * TN) {
         const int s_end = std::min(S, s0 + g.nt * TN);
         const int nt = ceil_div(s_end - s0, TN);
         WUST_CUDA(cudaMemsetAsync(sync, 0, sizeof(unsigned) * g.sync_words, st));
-        if (adjoint) WUST_CUDA(cudaMemsetAsync(tmp, 0, sizeof(float2) * g.tmp_elems, st));
         p.s0 = s0;
         p.s_end = s_end;
         p.group_ctr = sync;
-        p.tile_ctr = sync + g.nt;
         const dim3 grid(g.mt, nt, g.ks);
         if (adjoint) launch_sweep<true>(p, grid, st);
         else launch_sweep<false>(p, grid, st);
