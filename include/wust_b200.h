@@ -197,6 +197,13 @@ int wust_solver_curvature(wust_solver *s, const double *direction, double *curva
 int wust_solver_stats(const wust_solver *s, int *refine_iters, double *final_residual,
                       double *error_estimate, long long *kernel_launches);
 
+/* Counters of the last factorization (no counterpart in the reference, which
+ * always runs cuSOLVER LU per page): out[0] tensor-core GEMMs and out[1] X
+ * updates of the Newton-Schulz pages, out[2] pages inverted by Newton-Schulz,
+ * out[3] pages inverted by Gauss-Jordan.  Profiles other than
+ * WUST_PRECISION_TF32_REFINED report {0, 0, 0, Nx}. */
+int wust_solver_factor_stats(const wust_solver *s, long long out[4]);
+
 /* Self-test of the bounded device-side wait used by the persistent kernels
  * (no counterpart in the reference, whose MEX calls are synchronous library
  * calls): one CTA waits at a grid barrier that can never fill; the wait must

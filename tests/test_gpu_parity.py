@@ -163,6 +163,35 @@ def test_tensor_core_sweep_split_k_and_source_batches():
         assert rel(a, b) < 1e-7, adjoint
 
 
+def test_newton_schulz_factor_agrees_with_gauss_jordan():
+    """The TF32 profile's Schur inverses (Newton-Schulz iterations on the
+    tensor cores, Gauss-Jordan on the pages where the previous inverse is no
+    start) agree with the complex-single Gauss-Jordan pages to TF32 accuracy,
+    on a textured medium where the iteration needs several steps."""
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    ny = nx = 330
+    dx = 0.3e-3
+    x = (np.arange(nx) - (nx - 1) / 2) * dx
+    y = (np.arange(ny) - (ny - 1) / 2) * dx
+    X, Y = np.meshgrid(x, y)
+    rng = np.random.default_rng(5)
+    c = 1500 + 60 * np.exp(-((X - 4e-3) ** 2 + Y ** 2) / (2 * (15e-3) ** 2)) + 5 * rng.standard_normal(X.shape)
+    opts = dict(backend="gpu", stencil_bounds=(1400, 1700))
+    ref = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, 16 * dx, opts, precision="c64", max_sources=4)
+    tc = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, 16 * dx, opts, precision="tf32-refined", max_sources=4)
+    a = to_np(ref.block("invT"))
+    b = to_np(tc.block("invT"))
+    st = tc.factor_stats()
+    assert st["newton_schulz_pages"] + st["gauss_jordan_pages"] == nx, st
+    assert st["newton_schulz_pages"] >= nx // 2, st
+    assert st["gemms"] >= 2 * st["newton_schulz_pages"] - nx, st
+    per_page = np.linalg.norm((b - a).reshape(-1, nx), axis=0) / np.linalg.norm(a.reshape(-1, nx), axis=0)
+    assert per_page.max() < 5e-3, (per_page.argmax(), per_page.max())
+    assert rel(b, a) < 2e-3
+    ref.close()
+    tc.close()
+
+
 def test_mass_apply_matches_oracle(small):
     p, ref = small
     s = make_gpu_solver(p, p.c_true, p.frequencies_hz[0])

@@ -30,7 +30,7 @@ EXPORTED = (
     "wust_decomp_block_lu", "wust_decomp_block_lu_noalloc", "wust_apply_block_lu",
     "wust_solver_create", "wust_solver_refactor", "wust_solver_destroy", "wust_solver_timings",
     "wust_solver_stencil", "wust_solver_block", "wust_solver_solve", "wust_solver_mass_apply",
-    "wust_solver_oracle", "wust_solver_curvature", "wust_solver_stats",
+    "wust_solver_oracle", "wust_solver_curvature", "wust_solver_stats", "wust_solver_factor_stats",
     "wust_selftest_barrier_timeout",
 )
 
@@ -88,6 +88,7 @@ def load() -> C.CDLL:
     lib.wust_solver_oracle.argtypes = [vp, vp, i, vp, i, vp, vp, i, i, pd, vp]
     lib.wust_solver_curvature.argtypes = [vp, vp, pd]
     lib.wust_solver_stats.argtypes = [vp, pi, pd, pd, C.POINTER(C.c_longlong)]
+    lib.wust_solver_factor_stats.argtypes = [vp, C.POINTER(C.c_longlong)]
     lib.wust_selftest_barrier_timeout.argtypes = [i, pi]
     for name in EXPORTED:
         if name not in ("wust_status_id", "wust_last_error"):

@@ -138,6 +138,10 @@ struct wust_solver {
     unsigned *tc_sync = nullptr;
     int *tc_err = nullptr;
     TcSweepGeom tc_geom{};
+    // Newton-Schulz factorization (TF32 profile)
+    void *ns_scratch = nullptr;
+    NsGeom ns_g{};
+    long long ns_stats[4] = {};       // GEMMs, X updates, Newton-Schulz pages, Gauss-Jordan pages
     float2 *stage_c = nullptr; size_t stage_c_cap = 0;
     double assembly_ms = 0, factor_ms = 0;
     int last_refine_iters = 0;
@@ -179,7 +183,7 @@ static void free_solver(wust_solver *s) {
     void *ptrs[] = {s->vel, s->atten, s->exi, s->eyi, s->mult, s->status, s->invT, s->fscratch, s->u, s->lam,
                     s->tmp, s->work, s->x64, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
                     s->rx_at, s->Yd, s->maskd, s->resid, s->scale, s->loss_src, s->grad, s->dir, s->ret_u,
-                    s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err};
+                    s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err, s->ns_scratch};
     for (void *p : ptrs) dfree(p);
     for (int i = 0; i < 9; ++i) { dfree(s->c128[i]); dfree(s->c64[i]); }
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
@@ -239,7 +243,22 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
     assemble_launch(in, s->vel, atten_dev, s->exi, s->eyi, s->c128, s->c64, s->mult, s->status, st);
     WUST_CUDA(cudaEventRecord(s->ev[1], st));
     int hstat[3] = {0, 0, 0};
-    factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
+    auto check_assembly = [&](int astat) {
+        if (astat == 1) fail(WUST_ERR_INVALID_INPUT, "Expected a positive finite [ny,nx] medium");
+        if (astat == 2) fail(WUST_ERR_INVALID_INPUT, "k-Wave local dispersion target is evanescent");
+        if (astat == 3) fail(WUST_ERR_NUMERICAL_FAILURE, "LDR-9 produced invalid wavenumber or derivative");
+    };
+    if (s->precision == WUST_PRECISION_TF32_REFINED && s->ns_scratch) {
+        // the iteration needs a valid operator: check the assembly first
+        int astat0 = 0;
+        WUST_CUDA(cudaMemcpyAsync(&astat0, s->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+        WUST_CUDA(cudaStreamSynchronize(st));
+        check_assembly(astat0);
+        for (long long &v : s->ns_stats) v = 0;
+        ns_factor(s->coefs64(), s->invT, s->ns_g, s->ns_scratch, s->fscratch, s->fscratch_bytes, st, s->ns_stats);
+    } else {
+        factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
+    }
     if (s->precision == WUST_PRECISION_TF32_REFINED)
         tc_pack_invT(s->invT, s->ny, s->nx, s->tc_geom, s->tc_afwd, s->tc_aadj, st);
     WUST_CUDA(cudaEventRecord(s->ev[2], st));
@@ -252,9 +271,7 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
     s->assembly_ms = ms0;
     s->factor_ms = ms1;
     s->ret_valid = 0;
-    if (astat == 1) fail(WUST_ERR_INVALID_INPUT, "Expected a positive finite [ny,nx] medium");
-    if (astat == 2) fail(WUST_ERR_INVALID_INPUT, "k-Wave local dispersion target is evanescent");
-    if (astat == 3) fail(WUST_ERR_NUMERICAL_FAILURE, "LDR-9 produced invalid wavenumber or derivative");
+    check_assembly(astat);
     if (hstat[2]) fail(WUST_ERR_DEVICE_TIMEOUT, "factorization grid barrier %d timed out", hstat[2]);
     if (hstat[0]) fail(WUST_ERR_SINGULAR_SCHUR_BLOCK, "Schur block %d is singular at pivot %d", hstat[0], hstat[1] + 1);
 }
@@ -559,6 +576,8 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
             s->tc_b = dalloc<uint8_t>(s->tc_geom.b_bytes);
             s->tc_part = dalloc<float>(s->tc_geom.part_bytes / sizeof(float));
             s->tc_sync = dalloc<unsigned>(s->tc_geom.sync_words);
+            s->ns_g = ns_geom(ny, ns_max_ctas());
+            if (s->ns_g.ks > 0) WUST_CUDA(cudaMalloc(&s->ns_scratch, s->ns_g.scratch_bytes));
             s->tc_err = dalloc<int>(4);
             WUST_CUDA(cudaMemset(s->tc_err, 0, 4 * sizeof(int)));
         }
@@ -804,6 +823,18 @@ int wust_solver_stats(const wust_solver *s, int *refine_iters, double *final_res
         if (final_residual) *final_residual = s->last_residual;
         if (error_estimate) *error_estimate = s->last_error_est;
         if (kernel_launches) *kernel_launches = s->launches;
+    });
+}
+
+int wust_solver_factor_stats(const wust_solver *s, long long out[4]) {
+    return guarded([&] {
+        if (!s || !out) fail(WUST_ERR_INVALID_INPUT, "null solver or output");
+        if (s->precision == WUST_PRECISION_TF32_REFINED && s->ns_scratch) {
+            for (int i = 0; i < 4; ++i) out[i] = s->ns_stats[i];
+        } else {
+            out[0] = out[1] = out[2] = 0;
+            out[3] = s->nx;
+        }
     });
 }
 

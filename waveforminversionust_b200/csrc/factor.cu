@@ -44,6 +44,7 @@ struct FactorParams {
     int *err;              // barrier timeout site
     int *status;           // [0]: 1 + first page with a bad pivot; [1]: pivot index
     int n, n_pad;
+    int j0, j1;            // pages [j0, j1); page j0 - 1 (if any) is already in invT
     unsigned long long timeout_ns;
 #ifdef WUST_FACTOR_PROFILE
     unsigned long long *prof;   // [0] prologue, [1] pivot block, [2] tile work, [3] barriers (block 0, ns)
@@ -216,8 +217,8 @@ __global__ void __launch_bounds__(GT, 1) factor_kernel(FactorParams p) {
 
     // Border rows/columns of every page are zero (decompBlockLU.cu:284-288).
     const size_t gstride = (size_t)gridDim.x * blockDim.x;
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + tid; idx < (size_t)nx * 4 * ny; idx += gstride) {
-        const size_t page = idx / (4 * (size_t)ny);
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + tid; idx < (size_t)(p.j1 - p.j0) * 4 * ny; idx += gstride) {
+        const size_t page = p.j0 + idx / (4 * (size_t)ny);
         const int rem = (int)(idx % (4 * (size_t)ny));
         const int which = rem / ny, k = rem % ny;
         const size_t off = which == 0 ? (size_t)ny * k
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(GT, 1) factor_kernel(FactorParams p) {
         p.invT[page * page_sz + off] = make_float2(0.f, 0.f);
     }
 
-    for (int j = 0; j < nx; ++j) {
+    for (int j = p.j0; j < p.j1; ++j) {
         // ---- prologue: ws0 = T_j interior (identity padding) ----------------
         const float2 *X = p.invT + (size_t)(j > 0 ? j - 1 : 0) * page_sz;
         for (int t = blockIdx.x; t < nt * nt; t += gridDim.x) {
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(GT, 1) factor_kernel(FactorParams p) {
 size_t factor_scratch_bytes(int ny) { return factor_scratch_bytes_for(ny); }
 
 void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t scratch_bytes,
-                   cudaStream_t stream, double timeout_s, int *host_status) {
+                   cudaStream_t stream, double timeout_s, int *host_status, int j0, int j1) {
     const int ny = co.ny;
     const int n = ny - 2;
     const int np_ = (int)factor_pad(ny);
@@ -375,6 +376,9 @@ void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t 
     p.status = tail + 2;
     p.n = n;
     p.n_pad = np_;
+    p.j0 = j0;
+    p.j1 = j1 < 0 ? co.nx : j1;
+    if (p.j0 < 0 || p.j0 >= p.j1 || p.j1 > co.nx) fail(WUST_ERR_RUNTIME, "factor page range [%d, %d) invalid", j0, j1);
     p.timeout_ns = (unsigned long long)(timeout_s * 1e9);
     WUST_CUDA(cudaMemsetAsync(tail, 0, 8 * sizeof(int), stream));
 

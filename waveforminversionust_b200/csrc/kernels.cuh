@@ -15,9 +15,10 @@ constexpr size_t factor_pad(int ny) { return ((size_t)(ny - 2) + kFactorTile - 1
 constexpr size_t factor_scratch_bytes_for(int ny) { return 2 * factor_pad(ny) * factor_pad(ny) * 8 + 256; }
 size_t factor_scratch_bytes(int ny);
 // host_status (nullable, int[3]): {1+bad page, pivot, barrier timeout site};
-// when non-null the call synchronizes the stream.
+// when non-null the call synchronizes the stream.  Pages [j0, j1) are
+// factored (j1 < 0: through the last page); page j0 - 1 must already be in invT.
 void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t scratch_bytes,
-                   cudaStream_t stream, double timeout_s, int *host_status);
+                   cudaStream_t stream, double timeout_s, int *host_status, int j0 = 0, int j1 = -1);
 int barrier_selftest(double timeout_s, int *site_out);
 
 // ---- sweep.cu --------------------------------------------------------------
@@ -50,6 +51,20 @@ void tc_pack_invT(const float2 *invT, int ny, int nx, const TcSweepGeom &g, uint
 void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcSweepGeom &g,
                     const SrcView &src, int S, bool adjoint, float2 *u, uint8_t *bglob, float *part, unsigned *sync,
                     int *err, cudaStream_t st);
+
+// ---- nsfactor.cu (Newton-Schulz Schur inverses, TF32 tensor cores) ---------
+struct NsGeom {
+    int n, mt, ntn, kc, ks, per;   // ks == 0: the grid does not fit; Gauss-Jordan only
+    size_t a_bytes, b_bytes, part_bytes, scratch_bytes;
+};
+NsGeom ns_geom(int ny, int max_ctas);
+int ns_max_ctas();
+// All pages of invT: Newton-Schulz where the previous page is a good start,
+// the Gauss-Jordan kernel elsewhere (gj_scratch as for factor_launch).
+// stats (nullable, long long[4]): GEMMs, X updates, Newton-Schulz pages,
+// Gauss-Jordan pages (accumulated).
+void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats);
 
 // ---- assemble.cu -----------------------------------------------------------
 struct AssemblyInput {

@@ -1,0 +1,528 @@
+// Schur inverses of decompBlockLU (Runtime/solver/decompBlockLU.cu:337-368)
+// by Newton-Schulz iteration on the tensor cores, for the refined TF32
+// profile (whose FP64-residual refinement absorbs the TF32 error of the
+// factor, as it does that of the sweeps).
+//
+// Adjacent Schur complements of the Helmholtz operator differ little: with
+// X_0 = invT_{j-1}, the residual R_0 = I - T_j X_0 of the interior columns
+// has an RMS singular value of 1e-3 (homogeneous medium) to 0.3 (tissue
+// texture).  Newton-Schulz squares it every iteration:
+//     R_k = I - T_j X_k,     X_{k+1} = X_k + X_k R_k,     R_{k+1} = R_k^2,
+// so one to four iterations (two complex GEMMs each) replace the O(n)
+// sequential pivot steps of Gauss-Jordan.  Per column, with r_k the RMS of
+// R_k (||R_k||_F / sqrt(n), summed in a fixed order so every CTA decides
+// alike):
+//     r_k <= kAccept                      accept X_k
+//     r_k <= kLastUpdate, or stalled      one more update, accept
+//     diverging / not contracting         give the column back (Gauss-Jordan)
+// Columns where X_{j-1} is no start (the Dirichlet columns, the first
+// columns after them) go to the Gauss-Jordan kernel; the host driver
+// alternates between the two.
+//
+// Both products are n x n x n complex GEMMs, split into one real GEMM with
+// re/im interleaved along K (rows 0-63 of a 128-row A tile give the real
+// parts of 64 complex rows, rows 64-127 the imaginary parts):
+//     A = [Yr -Yi; Yi Yr] packed per (64-row tile, 16-column K chunk),
+//     B = complex columns of Z packed per (112-column tile, K chunk).
+// Grid: 64-row tiles x 112-column tiles x ks K slices, one CTA per SM,
+// launched cooperatively; operands stream through a shared-memory ring with
+// cp.async.bulk; each CTA's TF32 partial tile goes to L2 and, after a grid
+// barrier, the CTAs of a tile each sum one row slice in rank order and
+// write the epilogue (R in B layout, or X in A, B and fp32 layouts).
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "tc.cuh"
+
+namespace wust {
+
+using tc::chunk_off;
+using tc::to_tf32;
+
+namespace {
+
+constexpr int NTN = 112;                           // MMA N: complex columns per tile
+constexpr int kRows = 64;                          // complex rows per M tile
+constexpr int kKRows = 16;                         // complex K rows per chunk
+constexpr int kStages = 7;
+constexpr int kNsThreads = 256;
+constexpr int kBChunkNs = NTN * tc::kChunkBytes;   // 14 KB
+constexpr int kStageBytes = tc::kAChunk + kBChunkNs;
+constexpr size_t kNsSmem = (size_t)kStages * kStageBytes + 512;
+static_assert(kNsSmem <= 232448, "shared memory of one CTA");
+constexpr int kTmemCols = 128;
+
+constexpr float kAccept = 2e-4f;        // residual small enough: keep X_k
+constexpr float kLastUpdate = 2e-3f;    // one more update reaches the TF32 floor
+constexpr float kFirstFail = 0.8f;      // X_{j-1} is no start for this column
+constexpr float kStallAccept = 0.05f;   // stalled at this level: finish with one update
+
+enum { NS_SITE_COPY = 21, NS_SITE_MMA = 22, NS_SITE_SYNC = 23 };
+
+}  // namespace
+
+struct NsParams {
+    Coefs<float2> co;
+    float2 *invT;            // [ny, ny, nx] column-major pages
+    float2 *xf;              // current X, fp32 complex, column-major n x n
+    uint8_t *aT, *aX;        // A-packed T_j and X: [mt][kc] x 16 KB
+    uint8_t *bX, *bR;        // B-packed X and R:   [ntn][kc] x 14 KB
+    float *part;             // [tile][ks][128][NTN]
+    double *rn;              // [nblocks] per-CTA sums of |R|^2
+    unsigned *ctr;           // grid barrier counter
+    int *err;                // wait-site code
+    int *status;             // [0] failed column or -1, [1] GEMMs, [2] updates, [3] columns done
+    int ny, nx, n, mt, ntn, kc, ks, per;
+    int j0, j1, max_iter;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ bool ns_sync(unsigned *ctr, unsigned target, int *err, int *s_ok,
+                                        unsigned long long timeout_ns) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(ctr), "r"(1u) : "memory");
+        int ok = 1;
+        const unsigned long long t0 = global_timer_ns();
+        for (unsigned spin = 0;; ++spin) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+            if ((int)(v - target) >= 0) break;
+            if ((spin & 15u) == 15u) {
+                if (*(volatile int *)err) { ok = 0; break; }
+                if (global_timer_ns() - t0 > timeout_ns) {
+                    atomicCAS(err, 0, NS_SITE_SYNC);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// X(r, c) into the A layout (two stacked rows) and the B layout.
+__device__ __forceinline__ void put_x_packed(const NsParams &p, uint8_t *aX, uint8_t *bX, int r, int c, float2 v) {
+    const float xr = to_tf32(v.x), xi = to_tf32(v.y);
+    uint8_t *ac = aX + ((size_t)(r / kRows) * p.kc + c / kKRows) * tc::kAChunk;
+    const int ke = 2 * (c % kKRows);
+    *reinterpret_cast<float2 *>(ac + chunk_off(r % kRows, ke)) = make_float2(xr, -xi);
+    *reinterpret_cast<float2 *>(ac + chunk_off(r % kRows + kRows, ke)) = make_float2(xi, xr);
+    uint8_t *bc = bX + ((size_t)(c / NTN) * p.kc + r / kKRows) * kBChunkNs;
+    *reinterpret_cast<float2 *>(bc + chunk_off(c % NTN, 2 * (r % kKRows))) = make_float2(xr, xi);
+}
+
+__global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *misc = smem + (size_t)kStages * kStageBytes;
+    uint64_t *full = reinterpret_cast<uint64_t *>(misc);
+    uint64_t *empty = full + kStages;
+    uint64_t *done = empty + kStages;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(misc + 128);
+    int *s_ok = reinterpret_cast<int *>(misc + 132);
+    int *s_dec = reinterpret_cast<int *>(misc + 136);        // decision, r_k
+    double *s_red = reinterpret_cast<double *>(misc + 192);  // one per warp
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int mt = blockIdx.x, nb = blockIdx.y, ks = blockIdx.z;
+    const int KS = p.ks;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const int nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const int ny = p.ny, n = p.n;
+    const size_t page_sz = (size_t)ny * ny;
+    const int tile = mt + p.mt * nb;
+    const int c0 = ks * p.per;
+    const int nch = max(0, min(p.kc, c0 + p.per) - c0);
+    const int gthreads = nblocks * kNsThreads;
+    const int gtid = bid * kNsThreads + tid;
+    unsigned epoch = 0;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(done, 1);
+        tc::mbar_fence_init();
+    }
+    if (warp == 0) tc::tmem_alloc(tmem_slot, kTmemCols);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    uint32_t u_issue = 0, u_cons = 0;    // ring counters (thread 0)
+    uint32_t n_gemm = 0;                 // GEMMs run (done-barrier phase)
+    bool ok = true;
+
+    // One GEMM C = Apack * Bpack^T over this CTA's K slice into TMEM, then
+    // the partial tile into L2.  Returns false on an expired wait.
+    auto gemm = [&](const uint8_t *Apack, const uint8_t *Bpack) -> bool {
+        if (tid == 0) {
+            const uint8_t *ab = Apack + ((size_t)mt * p.kc + c0) * tc::kAChunk;
+            const uint8_t *bb = Bpack + ((size_t)nb * p.kc + c0) * kBChunkNs;
+            bool good = true;
+            auto issue = [&](int c) {
+                const uint32_t s = u_issue % kStages, f = u_issue / kStages;
+                if (f >= 1 && !tc::mbar_wait(&empty[s], (f - 1) & 1u, p.timeout_ns)) good = false;
+                uint8_t *st = smem + (size_t)s * kStageBytes;
+                tc::mbar_expect_tx(&full[s], kStageBytes);
+                tc::bulk_g2s(st, ab + (size_t)c * tc::kAChunk, tc::kAChunk, &full[s]);
+                tc::bulk_g2s(st + tc::kAChunk, bb + (size_t)c * kBChunkNs, kBChunkNs, &full[s]);
+                ++u_issue;
+            };
+            // kStages - 1 chunks ahead; chunk c + kStages - 1 refills the stage
+            // of chunk c - 1, whose MMAs were issued one chunk earlier
+            for (int c = 0; c < nch && c < kStages - 1; ++c) issue(c);
+            constexpr uint32_t kIdesc = tc::instr_desc<true>(tc::kTileRows, NTN);
+            for (int c = 0; c < nch; ++c) {
+                const uint32_t s = u_cons % kStages, f = u_cons / kStages;
+                if (!tc::mbar_wait(&full[s], f & 1u, p.timeout_ns)) { good = false; }
+                ++u_cons;
+                tc::fence_after();
+                const uint8_t *st = smem + (size_t)s * kStageBytes;
+#pragma unroll
+                for (int k = 0; k < tc::kChunkBytes / 32; ++k)
+                    tc::mma<true>(tmem, tc::smem_desc(st + k * 256), tc::smem_desc(st + tc::kAChunk + k * 256), kIdesc,
+                                  (c > 0 || k > 0) ? 1u : 0u);
+                tc::commit(&empty[s]);
+                if (c + kStages - 1 < nch) issue(c + kStages - 1);
+            }
+            tc::commit(done);
+            if (!good) atomicCAS(p.err, 0, NS_SITE_COPY);
+        }
+        if (!tc::mbar_wait(done, n_gemm & 1u, p.timeout_ns)) atomicCAS(p.err, 0, NS_SITE_MMA);
+        ++n_gemm;
+        tc::fence_after();
+        // partial tile: warp w reads TMEM lanes 32(w%4).., columns half (w/4)
+        const int row = 32 * (warp & 3) + lane;
+        const int cb0 = (NTN / 2) * (warp >> 2);
+        float *mypart = p.part + ((size_t)(tile * KS + ks) * 128 + row) * NTN + cb0;
+#pragma unroll
+        for (int cb = 0; cb < NTN / 2; cb += 8) {
+            float t[8];
+            if (nch > 0) {
+                tc::tmem_ld8(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(cb0 + cb), t);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) t[q] = 0.f;
+            }
+            __stcg(reinterpret_cast<float4 *>(mypart + cb), make_float4(t[0], t[1], t[2], t[3]));
+            __stcg(reinterpret_cast<float4 *>(mypart + cb + 4), make_float4(t[4], t[5], t[6], t[7]));
+        }
+        tc::fence_before();
+        epoch += (unsigned)nblocks;
+        return ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns);
+    };
+
+    // Rows of this tile whose split-K sum this CTA forms.
+    const int rows_per = (kRows + KS - 1) / KS;
+    const int rbeg = ks * rows_per, rend = min(kRows, rbeg + rows_per);
+    auto tile_value = [&](int rl, int cl) -> float2 {
+        const float *pt = p.part + (size_t)tile * KS * 128 * NTN + (size_t)rl * NTN + cl;
+        float2 v = make_float2(0.f, 0.f);
+        for (int q = 0; q < KS; ++q) {
+            v.x += __ldcg(pt + (size_t)q * 128 * NTN);
+            v.y += __ldcg(pt + (size_t)q * 128 * NTN + (size_t)kRows * NTN);
+        }
+        return v;
+    };
+
+    // ---- start: X = invT_{j0-1} into the fp32 and packed copies; zero the
+    //      borders of the pages this launch writes ----------------------------
+    {
+        const float2 *X = p.invT + (size_t)(p.j0 - 1) * page_sz;
+        for (int idx = gtid; idx < n * n; idx += gthreads) {
+            const int r = idx % n, c = idx / n;
+            const float2 v = X[(size_t)(r + 1) + (size_t)ny * (c + 1)];
+            p.xf[idx] = v;
+            put_x_packed(p, p.aX, p.bX, r, c, v);
+        }
+        for (size_t idx = gtid; idx < (size_t)(p.j1 - p.j0) * 4 * ny; idx += gthreads) {
+            const size_t page = p.j0 + idx / (4 * (size_t)ny);
+            const int rem = (int)(idx % (4 * (size_t)ny));
+            const int which = rem / ny, k = rem % ny;
+            const size_t off = which == 0 ? (size_t)ny * k
+                             : which == 1 ? (size_t)(ny - 1) + (size_t)ny * k
+                             : which == 2 ? (size_t)k
+                                          : (size_t)k + (size_t)ny * (ny - 1);
+            p.invT[page * page_sz + off] = make_float2(0.f, 0.f);
+        }
+        epoch += (unsigned)nblocks;
+        ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns);
+    }
+
+    int n_gemms = 0, n_updates = 0, failed = -1, cols_done = 0;
+    for (int j = p.j0; j < p.j1 && ok && failed < 0; ++j) {
+        // ---- T_j = D_j - L_{j-1} X U_{j-1}  (interior, A layout) ------------
+        {
+            const int jm = j - 1;
+            for (int idx = gtid; idx < n * n; idx += gthreads) {
+                const int r = idx % n, c = idx / n;
+                const int R = r + 1, C = c + 1;
+                float2 v = make_float2(0.f, 0.f);
+                if (R == C) v = p.co.dd(R, j);
+                else if (R == C + 1) v = p.co.dl(C, j);
+                else if (R + 1 == C) v = p.co.du(R, j);
+                const float2 udc = p.co.ud(C, jm), uuc = p.co.uu(C - 1, jm), ulc = p.co.ul(C, jm);
+                float2 right[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {                   // rows r-1, r, r+1 of X (zero outside)
+                    const int rr = r - 1 + d;
+                    float2 acc = make_float2(0.f, 0.f);
+                    if (rr >= 0 && rr < n) {
+                        const float2 *xc = p.xf + rr;
+                        acc = cmul(xc[(size_t)n * c], udc);
+                        if (c > 0) cfma(acc, xc[(size_t)n * (c - 1)], uuc);
+                        if (c < n - 1) cfma(acc, xc[(size_t)n * (c + 1)], ulc);
+                    }
+                    right[d] = acc;
+                }
+                float2 lr = cmul(p.co.ld(R, jm), right[1]);
+                cfma(lr, p.co.ll(R - 1, jm), right[0]);
+                cfma(lr, p.co.lu(R, jm), right[2]);
+                v = csub(v, lr);
+                uint8_t *ac = p.aT + ((size_t)(r / kRows) * p.kc + c / kKRows) * tc::kAChunk;
+                const int ke = 2 * (c % kKRows);
+                const float tr = to_tf32(v.x), ti = to_tf32(v.y);
+                *reinterpret_cast<float2 *>(ac + chunk_off(r % kRows, ke)) = make_float2(tr, -ti);
+                *reinterpret_cast<float2 *>(ac + chunk_off(r % kRows + kRows, ke)) = make_float2(ti, tr);
+            }
+            epoch += (unsigned)nblocks;
+            if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
+        }
+
+        float r_prev = 0.f;
+        bool accepted = false;
+        for (int k = 0; ok && !accepted && failed < 0; ++k) {
+            // ---- R_k = I - T X_k (B layout) and its squared norm -----------
+            if (!(ok = gemm(p.aT, p.bX))) break;
+            ++n_gemms;
+            double acc2 = 0.0;
+            for (int it = tid; it < (rend - rbeg) * NTN; it += kNsThreads) {
+                const int rl = rbeg + it / NTN, cl = it % NTN;
+                const int r = mt * kRows + rl, c = nb * NTN + cl;
+                if (r >= n || c >= n) continue;
+                const float2 pv = tile_value(rl, cl);
+                const float2 rv = make_float2((r == c ? 1.f : 0.f) - pv.x, -pv.y);
+                acc2 += (double)rv.x * rv.x + (double)rv.y * rv.y;
+                uint8_t *bc = p.bR + ((size_t)nb * p.kc + r / kKRows) * kBChunkNs;
+                *reinterpret_cast<float2 *>(bc + chunk_off(cl, 2 * (r % kKRows))) =
+                    make_float2(to_tf32(rv.x), to_tf32(rv.y));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc2 += __shfl_xor_sync(0xffffffffu, acc2, o);
+            if (lane == 0) s_red[warp] = acc2;
+            __syncthreads();
+            if (tid == 0) {
+                double t = 0.0;
+                for (int w = 0; w < kNsThreads / 32; ++w) t += s_red[w];
+                p.rn[bid] = t;
+            }
+            epoch += (unsigned)nblocks;
+            if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
+            // ---- decision (identical in every CTA: same sums, same order) ----
+            if (tid == 0) {
+                double t = 0.0;
+                for (int b = 0; b < nblocks; ++b) t += __ldcg(p.rn + b);
+                const float r_k = (float)sqrt(t / (double)n);
+                int dec;                          // 0 accept, 1 last update, 2 update, 3 fail
+                if (!(r_k == r_k) || r_k > 1e30f) dec = 3;
+                else if (r_k <= kAccept) dec = 0;
+                else if (r_k <= kLastUpdate) dec = 1;
+                else if (k > 0 && r_k >= r_prev) dec = 3;
+                else if (k > 0 && r_k > 0.3f * r_prev && r_k < kStallAccept) dec = 1;
+                else if ((k == 0 && r_k > kFirstFail) || k >= p.max_iter) dec = 3;
+                else dec = 2;
+                s_dec[0] = dec;
+                reinterpret_cast<float *>(s_dec)[1] = r_k;
+            }
+            __syncthreads();
+            const int dec = s_dec[0];
+            r_prev = reinterpret_cast<float *>(s_dec)[1];
+            __syncthreads();
+            if (dec == 3) {
+                failed = j;
+                break;
+            }
+            if (dec == 0) {
+                // X_k stays: copy it into page j
+                float2 *page = p.invT + (size_t)j * page_sz;
+                for (int idx = gtid; idx < n * n; idx += gthreads) {
+                    const int r = idx % n, c = idx / n;
+                    page[(size_t)(r + 1) + (size_t)ny * (c + 1)] = p.xf[idx];
+                }
+                accepted = true;
+                epoch += (unsigned)nblocks;
+                if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
+                break;
+            }
+            // ---- X_{k+1} = X_k + X_k R_k ------------------------------------
+            if (!(ok = gemm(p.aX, p.bR))) break;
+            ++n_gemms;
+            ++n_updates;
+            const bool last = (dec == 1);
+            float2 *page = p.invT + (size_t)j * page_sz;
+            for (int it = tid; it < (rend - rbeg) * NTN; it += kNsThreads) {
+                const int rl = rbeg + it / NTN, cl = it % NTN;
+                const int r = mt * kRows + rl, c = nb * NTN + cl;
+                if (r >= n || c >= n) continue;
+                const float2 pv = tile_value(rl, cl);
+                float2 *xp = p.xf + (size_t)r + (size_t)n * c;
+                const float2 xo = *xp;
+                const float2 xn = make_float2(xo.x + pv.x, xo.y + pv.y);
+                *xp = xn;
+                put_x_packed(p, p.aX, p.bX, r, c, xn);
+                if (last) page[(size_t)(r + 1) + (size_t)ny * (c + 1)] = xn;
+            }
+            epoch += (unsigned)nblocks;
+            if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
+            accepted = last;
+        }
+        if (accepted) ++cols_done;
+    }
+
+    if (bid == 0 && tid == 0) {
+        p.status[0] = failed;
+        p.status[1] = n_gemms;
+        p.status[2] = n_updates;
+        p.status[3] = cols_done;
+    }
+    // drain: every issued copy was consumed and every MMA committed (the
+    // ring waits even after an expired wait), so TMEM can go
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+}
+
+// ---------------------------------------------------------------------------
+NsGeom ns_geom(int ny, int max_ctas) {
+    NsGeom g{};
+    g.n = ny - 2;
+    g.mt = ceil_div(g.n, kRows);
+    g.ntn = ceil_div(g.n, NTN);
+    g.kc = ceil_div(g.n, kKRows);
+    const int tiles = g.mt * g.ntn;
+    g.ks = std::max(1, std::min(max_ctas / std::max(tiles, 1), 8));
+    g.ks = std::min(g.ks, g.kc);
+    if (tiles > max_ctas) g.ks = 0;          // does not fit: caller uses Gauss-Jordan only
+    g.per = g.ks > 0 ? ceil_div(g.kc, g.ks) : 0;
+    g.a_bytes = (size_t)g.mt * g.kc * tc::kAChunk;
+    g.b_bytes = (size_t)g.ntn * g.kc * kBChunkNs;
+    g.part_bytes = (size_t)tiles * std::max(g.ks, 1) * 128 * NTN * sizeof(float);
+    g.scratch_bytes = 2 * g.a_bytes + 2 * g.b_bytes + g.part_bytes + (size_t)g.n * g.n * sizeof(float2) +
+                      (size_t)max_ctas * sizeof(double) + 256;
+    return g;
+}
+
+int ns_max_ctas() {
+    static thread_local int configured_device = -1;
+    int dev = 0, sms = 0, per_sm = 0;
+    WUST_CUDA(cudaGetDevice(&dev));
+    if (configured_device != dev) {
+        WUST_CUDA(cudaFuncSetAttribute(ns_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNsSmem));
+        configured_device = dev;
+    }
+    WUST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    WUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ns_factor_kernel, kNsThreads, kNsSmem));
+    return sms * per_sm;
+}
+
+// Launch the Newton-Schulz pages [j0, j1); returns the first page it gave
+// back (or -1) and adds its GEMM/update counts to stats.
+static int ns_launch(const Coefs<float2> &co, float2 *invT, const NsGeom &g, uint8_t *scratch, int j0, int j1,
+                     cudaStream_t st, long long *stats) {
+    NsParams p;
+    p.co = co;
+    p.invT = invT;
+    uint8_t *q = scratch;
+    p.aT = q; q += g.a_bytes;
+    p.aX = q; q += g.a_bytes;
+    p.bX = q; q += g.b_bytes;
+    p.bR = q; q += g.b_bytes;
+    p.part = reinterpret_cast<float *>(q); q += g.part_bytes;
+    p.xf = reinterpret_cast<float2 *>(q); q += (size_t)g.n * g.n * sizeof(float2);
+    p.rn = reinterpret_cast<double *>(q); q += (size_t)g.mt * g.ntn * g.ks * sizeof(double);
+    int *tail = reinterpret_cast<int *>(scratch + g.scratch_bytes - 256);
+    p.ctr = reinterpret_cast<unsigned *>(tail);
+    p.err = tail + 1;
+    p.status = tail + 2;
+    p.ny = co.ny;
+    p.nx = co.nx;
+    p.n = g.n;
+    p.mt = g.mt;
+    p.ntn = g.ntn;
+    p.kc = g.kc;
+    p.ks = g.ks;
+    p.per = g.per;
+    p.j0 = j0;
+    p.j1 = j1;
+    p.max_iter = 8;
+    p.timeout_ns = 2000000000ull;
+    // packed operands: padding entries must be zero (never written later)
+    WUST_CUDA(cudaMemsetAsync(scratch, 0, 2 * g.a_bytes + 2 * g.b_bytes, st));
+    WUST_CUDA(cudaMemsetAsync(tail, 0, 8 * sizeof(int), st));
+    void *args[] = {&p};
+    WUST_CUDA(cudaLaunchCooperativeKernel((void *)ns_factor_kernel, dim3(g.mt, g.ntn, g.ks), dim3(kNsThreads), args,
+                                          kNsSmem, st));
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+    int h[6];
+    WUST_CUDA(cudaMemcpyAsync(h, tail, sizeof(h), cudaMemcpyDeviceToHost, st));
+    WUST_CUDA(cudaStreamSynchronize(st));
+    if (h[1]) fail(WUST_ERR_DEVICE_TIMEOUT, "Newton-Schulz factorization: device wait expired (site %d)", h[1]);
+    if (stats) {
+        stats[0] += h[3];
+        stats[1] += h[4];
+        stats[2] += h[5];
+    }
+    return h[2];
+}
+
+void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats) {
+    const int nx = co.nx;
+    int hstat[3];
+    auto gj = [&](int a, int b) {
+        factor_launch(co, invT, gj_scratch, gj_scratch_bytes, st, 10.0, hstat, a, b);
+        if (hstat[2]) fail(WUST_ERR_DEVICE_TIMEOUT, "factorization barrier timed out (site %d)", hstat[2]);
+        if (hstat[0])
+            fail(WUST_ERR_SINGULAR_SCHUR_BLOCK, "Schur block %d is singular (pivot %d)", hstat[0] - 1, hstat[1]);
+        if (stats) stats[3] += b - a;
+    };
+    // the first pages (Dirichlet column and the PML start) and the last one
+    // (Dirichlet column) have no usable predecessor
+    const int head = std::min(nx, 3);
+    if (g.ks <= 0 || nx <= head + 1) {
+        gj(0, nx);
+        return;
+    }
+    gj(0, head);
+    int j = head, fallbacks = 0;
+    while (j < nx - 1) {
+        if (fallbacks >= 16) {                  // not this operator's regime: finish with Gauss-Jordan
+            gj(j, nx - 1);
+            j = nx - 1;
+            break;
+        }
+        const int bad = ns_launch(co, invT, g, (uint8_t *)ns_scratch, j, nx - 1, st, stats);
+        if (bad < 0) {
+            j = nx - 1;
+        } else {
+            gj(bad, bad + 1);
+            ++fallbacks;
+            j = bad + 1;
+        }
+    }
+    gj(nx - 1, nx);
+}
+
+}  // namespace wust

@@ -32,6 +32,27 @@ constexpr int kAChunk = kTileRows * kChunkBytes; // 16 KB
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Byte offset of element (row, ke) inside one K chunk (128 bytes per row) of a
+// tile in the layout above.
+__host__ __device__ __forceinline__ size_t chunk_off(int row, int ke) {
+    return (size_t)(row >> 3) * kRowGroupBytes + (size_t)(ke >> 2) * 128 + (size_t)(row & 7) * 16 + (ke & 3) * 4;
+}
+
+// Round to TF32 (10-bit mantissa, nearest, ties away).  The tensor core
+// would otherwise drop the low mantissa bits of fp32 operands (truncation),
+// a bias that accumulates over long products.  Integer form (two ALU ops):
+// add half of the 13 dropped bits to the magnitude, clear them.  Inf and NaN
+// pass unchanged.
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t u = __float_as_uint(x);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    return __uint_as_float(u);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }

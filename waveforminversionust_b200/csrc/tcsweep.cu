@@ -57,21 +57,8 @@ constexpr size_t kSmemBar = 256;
 constexpr size_t kSweepSmem = kSmemA + kSmemB + kSmemBar;
 static_assert(kSweepSmem <= 232448, "shared memory of one CTA");
 
-// byte offset of element (row, ke) inside one chunk of a 128-row (or TN-row) tile
-__host__ __device__ __forceinline__ size_t chunk_off(int row, int ke) {
-    return (size_t)(row >> 3) * tc::kRowGroupBytes + (size_t)(ke >> 2) * 128 + (size_t)(row & 7) * 16 + (ke & 3) * 4;
-}
-
-// Round to TF32 (10-bit mantissa, nearest, ties away).  The tensor core
-// would otherwise drop the low mantissa bits of fp32 operands (truncation),
-// a bias that accumulates over the column sweep.  Integer form (two ALU
-// ops): add half of the 13 dropped bits to the magnitude, clear them.  Inf
-// and NaN pass unchanged.
-__device__ __forceinline__ float to_tf32(float x) {
-    uint32_t u = __float_as_uint(x);
-    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
-    return __uint_as_float(u);
-}
+using tc::chunk_off;
+using tc::to_tf32;
 
 TcSweepGeom tc_sweep_geom(int ny, int S, int max_ctas) {
     TcSweepGeom g{};
@@ -617,7 +604,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1) tc_sweep_kernel(SweepParams 
     // that will not come, then let them land (bounded)
     if (tid == 0 && a_step >= 0)
         for (int q = 0; q < nch; ++q) {
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&full[q])) : "memory");
+            tc::mbar_arrive(&full[q]);
             tc::mbar_wait(&full[q], (uint32_t)(a_step & 1), p.timeout_ns);
         }
     tc::fence_before();

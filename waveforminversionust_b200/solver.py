@@ -216,6 +216,12 @@ class HelmholtzSolver:
         return {"refine_iters": it.value, "final_residual": res.value, "error_estimate": err.value,
                 "kernel_launches": nl.value}
 
+    def factor_stats(self):
+        """How the last factorization inverted its Schur pages."""
+        out = (C.c_longlong * 4)()
+        check(self._lib.wust_solver_factor_stats(self._h, out))
+        return {"gemms": out[0], "updates": out[1], "newton_schulz_pages": out[2], "gauss_jordan_pages": out[3]}
+
 
 def decompBlockLU(Ld, Ll, Lu, Dd, Dl, Du, Ud, Ul, Uu, stream=None, timings=False):
     """Drop-in for the decompBlockLU MEX (decompBlockLU.cu:173-396) on CUDA tensors.
