@@ -205,7 +205,8 @@ def run_solves(args, p, solver_cls, torch):
     print(json.dumps(dict(mode="solve", precision=args.precision, workload=WORKLOADS[WORKLOAD]["text"],
                           ms_per_solve=ev0.elapsed_time(ev1) / args.steps, factor_ms=s.factor_seconds * 1e3,
                           refine_iters=st["refine_iters"], error_estimate=st["error_estimate"],
-                          final_residual=st["final_residual"], kernel_launches=st["kernel_launches"])), flush=True)
+                          final_residual=st["final_residual"], kernel_launches=st["kernel_launches"],
+                          factor_stats=s.factor_stats())), flush=True)
     s.close()
 
 

@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(GT, 1) factor_kernel(FactorParams p) {
     float2(*Cc)[G + 1] = Kr + 2 * NB;                                               // C[tile row][u], as Cc[u][row]
     float2(*Xs)[G + 3] = reinterpret_cast<float2(*)[G + 3]>(smem + 2 * kPivElems);   // prologue halo, Xs[col][row]
 
-    const int ny = p.co.ny, nx = p.co.nx, n = p.n, np_ = p.n_pad;
+    const int ny = p.co.ny, n = p.n, np_ = p.n_pad;
     const int nt = np_ / G, nsteps = np_ / NB;
     const unsigned nblocks = gridDim.x;
     const int tid = threadIdx.x, tr = tid % 16, tc = tid / 16;

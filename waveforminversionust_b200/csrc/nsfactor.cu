@@ -63,6 +63,28 @@ enum { NS_SITE_COPY = 21, NS_SITE_MMA = 22, NS_SITE_SYNC = 23 };
 
 }  // namespace
 
+// Optional phase timer (SM cycles of CTA 0, summed), profiling builds only.
+#ifdef WUST_NS_PROFILE
+__device__ unsigned long long g_ns_prof[16];
+#define NSPROF(k)                                                                                  \
+    do {                                                                                           \
+        if (bid == 0 && threadIdx.x == 0) {                                                        \
+            const long long t_ = clock64();                                                        \
+            g_ns_prof[k] += (unsigned long long)(t_ - prof_t);                                     \
+            prof_t = t_;                                                                           \
+        }                                                                                          \
+    } while (0)
+extern "C" int wust_ns_profile_read(unsigned long long *out) {
+    return (int)cudaMemcpyFromSymbol(out, g_ns_prof, sizeof(g_ns_prof));
+}
+extern "C" int wust_ns_profile_reset() {
+    unsigned long long z[16] = {};
+    return (int)cudaMemcpyToSymbol(g_ns_prof, z, sizeof(z));
+}
+#else
+#define NSPROF(k) ((void)0)
+#endif
+
 struct NsParams {
     Coefs<float2> co;
     float2 *invT;            // [ny, ny, nx] column-major pages
@@ -143,6 +165,9 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     const int gthreads = nblocks * kNsThreads;
     const int gtid = bid * kNsThreads + tid;
     unsigned epoch = 0;
+#ifdef WUST_NS_PROFILE
+    long long prof_t = clock64();
+#endif
 
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -165,6 +190,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     // One GEMM C = Apack * Bpack^T over this CTA's K slice into TMEM, then
     // the partial tile into L2.  Returns false on an expired wait.
     auto gemm = [&](const uint8_t *Apack, const uint8_t *Bpack) -> bool {
+        NSPROF(14);
         if (tid == 0) {
             const uint8_t *ab = Apack + ((size_t)mt * p.kc + c0) * tc::kAChunk;
             const uint8_t *bb = Bpack + ((size_t)nb * p.kc + c0) * kBChunkNs;
@@ -181,10 +207,12 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             // kStages - 1 chunks ahead; chunk c + kStages - 1 refills the stage
             // of chunk c - 1, whose MMAs were issued one chunk earlier
             for (int c = 0; c < nch && c < kStages - 1; ++c) issue(c);
+            NSPROF(12);
             constexpr uint32_t kIdesc = tc::instr_desc<true>(tc::kTileRows, NTN);
             for (int c = 0; c < nch; ++c) {
                 const uint32_t s = u_cons % kStages, f = u_cons / kStages;
                 if (!tc::mbar_wait(&full[s], f & 1u, p.timeout_ns)) { good = false; }
+                if (c == 0) NSPROF(11);
                 ++u_cons;
                 tc::fence_after();
                 const uint8_t *st = smem + (size_t)s * kStageBytes;
@@ -198,7 +226,9 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             tc::commit(done);
             if (!good) atomicCAS(p.err, 0, NS_SITE_COPY);
         }
+        NSPROF(1);
         if (!tc::mbar_wait(done, n_gemm & 1u, p.timeout_ns)) atomicCAS(p.err, 0, NS_SITE_MMA);
+        NSPROF(2);
         ++n_gemm;
         tc::fence_after();
         // partial tile: warp w reads TMEM lanes 32(w%4).., columns half (w/4)
@@ -218,21 +248,99 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             __stcg(reinterpret_cast<float4 *>(mypart + cb + 4), make_float4(t[4], t[5], t[6], t[7]));
         }
         tc::fence_before();
+        NSPROF(3);
         epoch += (unsigned)nblocks;
-        return ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns);
+        const bool synced = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns);
+        NSPROF(4);
+        return synced;
     };
 
     // Rows of this tile whose split-K sum this CTA forms.
-    const int rows_per = (kRows + KS - 1) / KS;
+    const int rows_per = ((kRows + KS - 1) / KS + 1) & ~1;   // even: B-layout units hold row pairs
     const int rbeg = ks * rows_per, rend = min(kRows, rbeg + rows_per);
-    auto tile_value = [&](int rl, int cl) -> float2 {
-        const float *pt = p.part + (size_t)tile * KS * 128 * NTN + (size_t)rl * NTN + cl;
-        float2 v = make_float2(0.f, 0.f);
+    // This CTA's epilogue items: item m of thread tid is it = tid + 256 m over
+    // the (rend - rbeg) x NTN slice; their split-K sums, with every load of a
+    // rank in flight at once.
+    constexpr int kEpi = ((kRows + 2) / 3 * NTN + kNsThreads - 1) / kNsThreads;   // bound for ks >= 3
+    const int n_items = (rend - rbeg) * NTN;
+    auto tile_values = [&](float2 (&v)[kEpi]) {
+        const float *pt = p.part + (size_t)tile * KS * 128 * NTN;
+#pragma unroll
+        for (int m = 0; m < kEpi; ++m) v[m] = make_float2(0.f, 0.f);
         for (int q = 0; q < KS; ++q) {
-            v.x += __ldcg(pt + (size_t)q * 128 * NTN);
-            v.y += __ldcg(pt + (size_t)q * 128 * NTN + (size_t)kRows * NTN);
+            const float *pq = pt + (size_t)q * 128 * NTN;
+#pragma unroll
+            for (int m = 0; m < kEpi; ++m) {
+                const int it = tid + kNsThreads * m;
+                if (it < n_items) {
+                    const int rl = rbeg + it / NTN, cl = it % NTN;
+                    v[m].x += __ldcg(pq + (size_t)rl * NTN + cl);
+                    v[m].y += __ldcg(pq + (size_t)(rl + kRows) * NTN + cl);
+                }
+            }
         }
-        return v;
+    };
+
+    // Staging of this CTA's slice (rows rbeg..rend-1 of the M tile, all NTN
+    // columns) in the operand ring, which is idle between GEMMs; from there
+    // every packed layout is written in whole 16-byte units.
+    constexpr int SP = NTN + 1;                                  // staged row pitch (float2)
+    float2 *sx = reinterpret_cast<float2 *>(smem);               // [rows_per][SP]
+    float2 *xw = reinterpret_cast<float2 *>(smem + 32768);       // Schur window [rows_per + 2][SP + 2]
+    const int nr = rend - rbeg;
+    const int grow0 = mt * kRows + rbeg;                         // global row of slice row 0
+    const int gcol0 = nb * NTN;
+    // A layout (rows i_s = r % 64 and r % 64 + 64, K units of two columns)
+    auto write_a = [&](uint8_t *Apack) {
+        for (int u = tid; u < nr * (NTN / 2); u += kNsThreads) {
+            const int rl = u % nr, cp = u / nr;
+            const int r = grow0 + rl, c = gcol0 + 2 * cp;
+            if (r >= n || c >= n) continue;
+            const float2 y0 = sx[rl * SP + 2 * cp];
+            const float2 y1 = c + 1 < n ? sx[rl * SP + 2 * cp + 1] : make_float2(0.f, 0.f);
+            uint8_t *ac = Apack + ((size_t)mt * p.kc + c / kKRows) * tc::kAChunk;
+            const int ke = 2 * (c % kKRows);
+            *reinterpret_cast<float4 *>(ac + chunk_off(r % kRows, ke)) =
+                make_float4(to_tf32(y0.x), -to_tf32(y0.y), to_tf32(y1.x), -to_tf32(y1.y));
+            *reinterpret_cast<float4 *>(ac + chunk_off(r % kRows + kRows, ke)) =
+                make_float4(to_tf32(y0.y), to_tf32(y0.x), to_tf32(y1.y), to_tf32(y1.x));
+        }
+    };
+    // B layout (column cl, K units of two rows)
+    auto write_b = [&](uint8_t *Bpack) {
+        for (int u = tid; u < (nr / 2) * NTN; u += kNsThreads) {
+            const int cl = u % NTN, rp = u / NTN;
+            const int r = grow0 + 2 * rp, c = gcol0 + cl;
+            if (r >= n || c >= n) continue;
+            const float2 z0 = sx[(2 * rp) * SP + cl];
+            const float2 z1 = r + 1 < n ? sx[(2 * rp + 1) * SP + cl] : make_float2(0.f, 0.f);
+            uint8_t *bc = Bpack + ((size_t)nb * p.kc + r / kKRows) * kBChunkNs;
+            *reinterpret_cast<float4 *>(bc + chunk_off(cl, 2 * (r % kKRows))) =
+                make_float4(to_tf32(z0.x), to_tf32(z0.y), to_tf32(z1.x), to_tf32(z1.y));
+        }
+    };
+    // column-major copy (leading dimension ld, element (r, c) at base[r + ld c])
+    auto write_cm = [&](float2 *base, size_t ld) {
+        for (int u = tid; u < nr * NTN; u += kNsThreads) {
+            const int rl = u % nr, cl = u / nr;
+            const int r = grow0 + rl, c = gcol0 + cl;
+            if (r < n && c < n) base[(size_t)r + ld * c] = sx[rl * SP + cl];
+        }
+    };
+    auto read_cm = [&](const float2 *base, size_t ld) {
+        float2 v[kEpi];                      // all loads first, then the stores
+#pragma unroll
+        for (int m = 0; m < kEpi; ++m) {
+            const int u = tid + kNsThreads * m;
+            const int rl = u % max(nr, 1), cl = u / max(nr, 1);
+            const int r = grow0 + rl, c = gcol0 + cl;
+            v[m] = (u < nr * NTN && r < n && c < n) ? base[(size_t)r + ld * c] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int m = 0; m < kEpi; ++m) {
+            const int u = tid + kNsThreads * m;
+            if (u < nr * NTN) sx[(u % nr) * SP + u / nr] = v[m];
+        }
     };
 
     // ---- start: X = invT_{j0-1} into the fp32 and packed copies; zero the
@@ -262,41 +370,93 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     int n_gemms = 0, n_updates = 0, failed = -1, cols_done = 0;
     for (int j = p.j0; j < p.j1 && ok && failed < 0; ++j) {
         // ---- T_j = D_j - L_{j-1} X U_{j-1}  (interior, A layout) ------------
+        NSPROF(0);
         {
+            // window of X_{j-1} around this CTA's slice and the slice's
+            // coefficients -> shared memory (all loads of a thread in flight)
             const int jm = j - 1;
-            for (int idx = gtid; idx < n * n; idx += gthreads) {
-                const int r = idx % n, c = idx / n;
-                const int R = r + 1, C = c + 1;
-                float2 v = make_float2(0.f, 0.f);
-                if (R == C) v = p.co.dd(R, j);
-                else if (R == C + 1) v = p.co.dl(C, j);
-                else if (R + 1 == C) v = p.co.du(R, j);
-                const float2 udc = p.co.ud(C, jm), uuc = p.co.uu(C - 1, jm), ulc = p.co.ul(C, jm);
-                float2 right[3];
+            const int wr = nr + 2, wc = NTN + 2;
+            float2 *cw_ = xw + (size_t)(kRows / 3 + 3) * (SP + 2);   // [3][NTN] column coefs ud, uu, ul
+            float2 *rw_ = cw_ + 3 * NTN;                            // [6][rows] row coefs ld, ll, lu, dd, dl, du
+            {
+                constexpr int kWin = ((kRows / 3 + 4) * (NTN + 2) + kNsThreads - 1) / kNsThreads;
+                float2 v[kWin];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {                   // rows r-1, r, r+1 of X (zero outside)
-                    const int rr = r - 1 + d;
-                    float2 acc = make_float2(0.f, 0.f);
-                    if (rr >= 0 && rr < n) {
-                        const float2 *xc = p.xf + rr;
-                        acc = cmul(xc[(size_t)n * c], udc);
-                        if (c > 0) cfma(acc, xc[(size_t)n * (c - 1)], uuc);
-                        if (c < n - 1) cfma(acc, xc[(size_t)n * (c + 1)], ulc);
-                    }
-                    right[d] = acc;
+                for (int m = 0; m < kWin; ++m) {
+                    const int u = tid + kNsThreads * m;
+                    const int rw = u % wr, cwi = u / wr;
+                    const int r = grow0 - 1 + rw, c = gcol0 - 1 + cwi;
+                    v[m] = (u < wr * wc && r >= 0 && r < n && c >= 0 && c < n) ? p.xf[(size_t)r + (size_t)n * c]
+                                                                                : make_float2(0.f, 0.f);
                 }
-                float2 lr = cmul(p.co.ld(R, jm), right[1]);
-                cfma(lr, p.co.ll(R - 1, jm), right[0]);
-                cfma(lr, p.co.lu(R, jm), right[2]);
-                v = csub(v, lr);
-                uint8_t *ac = p.aT + ((size_t)(r / kRows) * p.kc + c / kKRows) * tc::kAChunk;
-                const int ke = 2 * (c % kKRows);
-                const float tr = to_tf32(v.x), ti = to_tf32(v.y);
-                *reinterpret_cast<float2 *>(ac + chunk_off(r % kRows, ke)) = make_float2(tr, -ti);
-                *reinterpret_cast<float2 *>(ac + chunk_off(r % kRows + kRows, ke)) = make_float2(ti, tr);
+                // coefficients: items [0, 3 NTN) columns, [3 NTN, 3 NTN + 6 nr) rows
+                float2 cf[2];
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    const int q = tid + kNsThreads * m;
+                    float2 v2 = make_float2(0.f, 0.f);
+                    if (q < 3 * NTN) {
+                        const int which = q / NTN, cl = q % NTN, C = gcol0 + cl + 1;
+                        if (C <= n) v2 = which == 0 ? p.co.ud(C, jm) : which == 1 ? p.co.uu(C - 1, jm) : p.co.ul(C, jm);
+                    } else if (q < 3 * NTN + 6 * nr) {
+                        const int rt = q - 3 * NTN, which = rt / nr, rl = rt % nr, R = grow0 + rl + 1;
+                        if (R <= n) {
+                            if (which == 0) v2 = p.co.ld(R, jm);
+                            else if (which == 1) v2 = p.co.ll(R - 1, jm);
+                            else if (which == 2) v2 = p.co.lu(R, jm);
+                            else if (which == 3) v2 = p.co.dd(R, j);
+                            else if (which == 4) v2 = p.co.dl(R, j);        // element (R+1, R)
+                            else if (R >= 2) v2 = p.co.du(R - 1, j);        // element (R-1, R)
+                        }
+                    }
+                    cf[m] = v2;
+                }
+#pragma unroll
+                for (int m = 0; m < kWin; ++m) {
+                    const int u = tid + kNsThreads * m;
+                    if (u < wr * wc) xw[(u % wr) * (SP + 2) + u / wr] = v[m];
+                }
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    const int q = tid + kNsThreads * m;
+                    if (q < 3 * NTN + 6 * nr) cw_[q] = cf[m];       // rw_ follows cw_ directly
+                }
             }
+            __syncthreads();
+            for (int u = tid; u < nr * NTN; u += kNsThreads) {
+                const int cl = u % NTN, rl = u / NTN;
+                const int r = grow0 + rl, c = gcol0 + cl;
+                float2 v = make_float2(0.f, 0.f);
+                if (r < n && c < n) {
+                    // D_j(R, C): dd on the diagonal, dl(C) below (R = C+1), du(R) above (C = R+1)
+                    if (r == c) v = rw_[3 * nr + rl];
+                    else if (r == c + 1) v = rw_[4 * nr + (rl - 1 >= 0 ? rl - 1 : 0)];
+                    else if (r + 1 == c) v = rw_[5 * nr + (rl + 1 < nr ? rl + 1 : rl)];
+                    if (r == c + 1 && rl == 0) v = p.co.dl(c + 1, j);         // pair leaves the slice
+                    if (r + 1 == c && rl + 1 >= nr) v = p.co.du(r + 1, j);
+                    const float2 udc = cw_[cl], uuc = cw_[NTN + cl], ulc = cw_[2 * NTN + cl];
+                    float2 right[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {               // rows r-1, r, r+1 (window row rl + d)
+                        const float2 *xr = xw + (rl + d) * (SP + 2) + cl;    // columns c-1, c, c+1
+                        float2 acc = cmul(xr[1], udc);
+                        cfma(acc, xr[0], uuc);
+                        cfma(acc, xr[2], ulc);
+                        right[d] = acc;
+                    }
+                    float2 lr = cmul(rw_[rl], right[1]);
+                    cfma(lr, rw_[nr + rl], right[0]);
+                    cfma(lr, rw_[2 * nr + rl], right[2]);
+                    v = csub(v, lr);
+                }
+                sx[rl * SP + cl] = v;
+            }
+            __syncthreads();
+            write_a(p.aT);
+            NSPROF(5);
             epoch += (unsigned)nblocks;
             if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
+            NSPROF(6);
         }
 
         float r_prev = 0.f;
@@ -306,17 +466,25 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             if (!(ok = gemm(p.aT, p.bX))) break;
             ++n_gemms;
             double acc2 = 0.0;
-            for (int it = tid; it < (rend - rbeg) * NTN; it += kNsThreads) {
-                const int rl = rbeg + it / NTN, cl = it % NTN;
-                const int r = mt * kRows + rl, c = nb * NTN + cl;
-                if (r >= n || c >= n) continue;
-                const float2 pv = tile_value(rl, cl);
-                const float2 rv = make_float2((r == c ? 1.f : 0.f) - pv.x, -pv.y);
-                acc2 += (double)rv.x * rv.x + (double)rv.y * rv.y;
-                uint8_t *bc = p.bR + ((size_t)nb * p.kc + r / kKRows) * kBChunkNs;
-                *reinterpret_cast<float2 *>(bc + chunk_off(cl, 2 * (r % kKRows))) =
-                    make_float2(to_tf32(rv.x), to_tf32(rv.y));
+            NSPROF(0);
+            float2 pvs[kEpi];
+            tile_values(pvs);
+#pragma unroll
+            for (int m = 0; m < kEpi; ++m) {
+                const int it = tid + kNsThreads * m;
+                if (it >= n_items) break;
+                const int rl = it / NTN, cl = it % NTN;
+                const int r = grow0 + rl, c = gcol0 + cl;
+                float2 rv = make_float2(0.f, 0.f);
+                if (r < n && c < n) {
+                    const float2 pv = pvs[m];
+                    rv = make_float2((r == c ? 1.f : 0.f) - pv.x, -pv.y);
+                    acc2 += (double)rv.x * rv.x + (double)rv.y * rv.y;
+                }
+                sx[rl * SP + cl] = rv;
             }
+            __syncthreads();
+            write_b(p.bR);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc2 += __shfl_xor_sync(0xffffffffu, acc2, o);
             if (lane == 0) s_red[warp] = acc2;
@@ -326,12 +494,22 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 for (int w = 0; w < kNsThreads / 32; ++w) t += s_red[w];
                 p.rn[bid] = t;
             }
+            NSPROF(7);
             epoch += (unsigned)nblocks;
             if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
+            NSPROF(8);
             // ---- decision (identical in every CTA: same sums, same order) ----
+            {   // sum of the per-CTA norms: fixed tree, identical in every CTA
+                double v = 0.0;
+                for (int b2 = tid; b2 < nblocks; b2 += kNsThreads) v += __ldcg(p.rn + b2);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) s_red[warp] = v;
+                __syncthreads();
+            }
             if (tid == 0) {
                 double t = 0.0;
-                for (int b = 0; b < nblocks; ++b) t += __ldcg(p.rn + b);
+                for (int w = 0; w < kNsThreads / 32; ++w) t += s_red[w];
                 const float r_k = (float)sqrt(t / (double)n);
                 int dec;                          // 0 accept, 1 last update, 2 update, 3 fail
                 if (!(r_k == r_k) || r_k > 1e30f) dec = 3;
@@ -355,10 +533,9 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             if (dec == 0) {
                 // X_k stays: copy it into page j
                 float2 *page = p.invT + (size_t)j * page_sz;
-                for (int idx = gtid; idx < n * n; idx += gthreads) {
-                    const int r = idx % n, c = idx / n;
-                    page[(size_t)(r + 1) + (size_t)ny * (c + 1)] = p.xf[idx];
-                }
+                read_cm(p.xf, (size_t)n);
+                __syncthreads();
+                write_cm(page + ny + 1, (size_t)ny);
                 accepted = true;
                 epoch += (unsigned)nblocks;
                 if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
@@ -369,21 +546,29 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             ++n_gemms;
             ++n_updates;
             const bool last = (dec == 1);
+            NSPROF(0);
             float2 *page = p.invT + (size_t)j * page_sz;
-            for (int it = tid; it < (rend - rbeg) * NTN; it += kNsThreads) {
-                const int rl = rbeg + it / NTN, cl = it % NTN;
-                const int r = mt * kRows + rl, c = nb * NTN + cl;
-                if (r >= n || c >= n) continue;
-                const float2 pv = tile_value(rl, cl);
-                float2 *xp = p.xf + (size_t)r + (size_t)n * c;
-                const float2 xo = *xp;
-                const float2 xn = make_float2(xo.x + pv.x, xo.y + pv.y);
-                *xp = xn;
-                put_x_packed(p, p.aX, p.bX, r, c, xn);
-                if (last) page[(size_t)(r + 1) + (size_t)ny * (c + 1)] = xn;
+            read_cm(p.xf, (size_t)n);                  // X_k of the slice
+            float2 pvx[kEpi];
+            tile_values(pvx);
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < kEpi; ++m) {
+                const int it = tid + kNsThreads * m;
+                if (it >= n_items) break;
+                const int rl = it / NTN, cl = it % NTN;
+                float2 &x = sx[rl * SP + cl];
+                x = make_float2(x.x + pvx[m].x, x.y + pvx[m].y);
             }
+            __syncthreads();
+            write_cm(p.xf, (size_t)n);
+            if (last) write_cm(page + ny + 1, (size_t)ny);
+            write_a(p.aX);
+            write_b(p.bX);
+            NSPROF(9);
             epoch += (unsigned)nblocks;
             if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
+            NSPROF(10);
             accepted = last;
         }
         if (accepted) ++cols_done;
@@ -413,7 +598,7 @@ NsGeom ns_geom(int ny, int max_ctas) {
     const int tiles = g.mt * g.ntn;
     g.ks = std::max(1, std::min(max_ctas / std::max(tiles, 1), 8));
     g.ks = std::min(g.ks, g.kc);
-    if (tiles > max_ctas) g.ks = 0;          // does not fit: caller uses Gauss-Jordan only
+    if (g.ks < 3) g.ks = 0;                   // outside the epilogue bound: Gauss-Jordan only
     g.per = g.ks > 0 ? ceil_div(g.kc, g.ks) : 0;
     g.a_bytes = (size_t)g.mt * g.kc * tc::kAChunk;
     g.b_bytes = (size_t)g.ntn * g.kc * kBChunkNs;
