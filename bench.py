@@ -216,9 +216,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="c64-refined")
+    ap.add_argument("--precision", default="tf32-refined")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variants", default="c64", help="extra precision profiles timed beside the headline")
+    ap.add_argument("--variants", default="c64,c64-refined", help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
     ap.add_argument("--mode", default="gradient", choices=["gradient", "solve"],
                     help="solve: factor once, then time forward solves of all transmitters (kernel profiling)")
@@ -308,6 +308,7 @@ def main():
         barrier()
         fac_ms, launches = [], 0
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sw_ms0, sw_n0 = solver.sweep_times()
         with ClockSampler(local) as clk:
             barrier()
             ev0.record(stream)
@@ -318,11 +319,14 @@ def main():
             ev1.record(stream)
             barrier()
         dev_ms = max_over_ranks(ev0.elapsed_time(ev1))
+        sw_ms1, sw_n1 = solver.sweep_times()
         stats = solver.stats()
         res = dict(ms_per_step=dev_ms / args.steps, value=world * args.steps / (dev_ms * 1e-3),
                    factor_ms=float(np.mean(fac_ms)), launches_per_step=launches / args.steps,
                    refine_iters=stats["refine_iters"], final_residual=stats["final_residual"],
-                   loss=loss.value, clocks=clk.summary())
+                   loss=loss.value, clocks=clk.summary(),
+                   sweep_ms_per_launch=(sw_ms1 - sw_ms0) / max(sw_n1 - sw_n0, 1),
+                   sweeps_per_step=(sw_n1 - sw_n0) / args.steps, factor_stats=solver.factor_stats())
         if with_e2e:
             for _ in range(2):
                 step_host()
@@ -356,17 +360,32 @@ def main():
     except Exception:
         pass
     peak_tf = float(peaks.get("bf16_tflops", 1590.0))
-    fac_tflops = fl["factor"] / (head["factor_ms"] * 1e-3) / 1e12
-    roofline = dict(kernel="factor_kernel (Schur recursion + Gauss-Jordan inverses)", bound="tensor",
-                    achieved=fac_tflops, peak=peak_tf, unit="TFLOP/s", frac=fac_tflops / peak_tf,
-                    peak_source="MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1590 TFLOP/s",
-                    traffic=None, algorithmic_flop_per_launch=fl["factor"])
+    peak_src = ("MEASURED_PEAKS.json bf16_tflops (burst; the TF32 tensor rate of this part is half of it)"
+                if peaks else "fallback 1590 TFLOP/s")
+    # dominant kernel of the headline step: the sweep kernel (one launch = a
+    # forward + backward sweep pair over all sources) or the factorization
+    sweep_ms_step = head["sweep_ms_per_launch"] * head["sweeps_per_step"]
+    if sweep_ms_step >= head["factor_ms"]:
+        flop = fl["apply"]
+        achieved = flop / (head["sweep_ms_per_launch"] * 1e-3) / 1e12
+        kname = ("tc_sweep_kernel (persistent tcgen05 TF32 block-LU sweep pair, 256 sources)"
+                 if args.precision == "tf32-refined" else "sweep kernels (CUDA-core block-LU sweep pair)")
+    else:
+        flop = fl["factor"]
+        achieved = flop / (head["factor_ms"] * 1e-3) / 1e12
+        kname = ("ns_factor_kernel + factor_kernel (Newton-Schulz Schur inverses, Gauss-Jordan pages)"
+                 if args.precision == "tf32-refined" else "factor_kernel (Schur recursion + Gauss-Jordan inverses)")
+    roofline = dict(kernel=kname, bound="tensor", achieved=achieved, peak=peak_tf, unit="TFLOP/s",
+                    frac=achieved / peak_tf, peak_source=peak_src, traffic=None,
+                    algorithmic_flop_per_launch=flop,
+                    launch_ms=head["sweep_ms_per_launch"] if flop == fl["apply"] else head["factor_ms"])
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(p, n_solves=8)
     line = dict(metric="gradients_per_second", value=head["value"], unit="gradients/s", n_gpus=world,
                 steps=args.steps, warmup=args.warmup, ms_per_step=head["ms_per_step"], higher_is_better=True,
-                scaling="weak", vs_baseline=None, dtype="c64+c128-refine" if args.precision != "c64" else "c64",
+                scaling="weak", vs_baseline=None,
+                dtype={"c64": "c64", "c64-refined": "c64+c128-refine"}.get(args.precision, "tf32+c128-refine"),
                 data="synthetic",
                 config=dict(workload=WORKLOADS[WORKLOAD]["text"],
                             global_batch=N_TX * world, precision=args.precision, parallelism=f"replicas{world}",
@@ -374,6 +393,8 @@ def main():
                 e2e=head["e2e"], gpu_launches=int(round(head["launches_per_step"] * args.steps)),
                 roofline=roofline, clocks=head["clocks"],
                 detail=dict(factor_ms=head["factor_ms"], refine_iters=head["refine_iters"],
+                            sweep_ms_per_launch=head["sweep_ms_per_launch"], sweeps_per_step=head["sweeps_per_step"],
+                            factor_stats=head["factor_stats"],
                             final_relative_residual=head["final_residual"], flops=fl, variants=variants))
     if cpu:
         line["cpu_baseline"] = dict(value=cpu["value"], unit="gradients/s", cores=cpu["cores"], kind=cpu["kind"],

@@ -141,7 +141,14 @@ typedef struct {
     int refine_max_iters;          /* refined profiles: max refinement solves (0 -> 8) */
     double refine_tol;             /* refined profiles: relative FP64 residual target (0 -> 1e-5) */
     int max_sources;               /* largest RHS batch the object will see (0 -> 256) */
+    int factor_method;             /* WUST_FACTOR_*: how the Schur pages are inverted */
 } wust_solver_options;
+
+/* Schur-page inversion (no counterpart in the reference, which always uses
+ * cuSOLVER LU).  DEFAULT: Newton-Schulz on the tensor cores for the TF32
+ * profile, Gauss-Jordan otherwise; GAUSS_JORDAN: complex-single Gauss-Jordan
+ * for every profile (the TF32 profile then keeps tensor-core sweeps only). */
+enum wust_factor_method { WUST_FACTOR_DEFAULT = 0, WUST_FACTOR_GAUSS_JORDAN = 1 };
 
 /* Assemble the nine-point PML operator on the GPU and factorize it.
  * vel, atten: ny x nx (atten may be NULL = zero).  stream may be NULL. */
@@ -196,6 +203,14 @@ int wust_solver_curvature(wust_solver *s, const double *direction, double *curva
  * launches the call issued. */
 int wust_solver_stats(const wust_solver *s, int *refine_iters, double *final_residual,
                       double *error_estimate, long long *kernel_launches);
+
+/* Device time of the block-LU sweep pairs (one forward and one backward
+ * sweep over a batch of right-hand sides; refined solves run one per
+ * correction) since the solver was created, and their number (no counterpart
+ * in the reference).  Each pair is bracketed by events on the solver stream,
+ * so solves measure their sweeps at the cost of one stream synchronization
+ * per pair. */
+int wust_solver_sweep_times(const wust_solver *s, double *total_ms, long long *count);
 
 /* Counters of the last factorization (no counterpart in the reference, which
  * always runs cuSOLVER LU per page): out[0] tensor-core GEMMs and out[1] X

@@ -123,3 +123,18 @@ def test_package_without_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(ImportError):
         _lib.load()
+
+
+def test_mex_gateways_compile_against_api_declarations():
+    """The decompBlockLU / applyBlockLU MEX gateways compile as C99 against the
+    library header and declarations of the MATLAB MEX API they use."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if not gcc:
+        pytest.skip("gcc absent")
+    here = os.path.dirname(os.path.abspath(__file__))
+    mex_dir = os.path.join(os.path.dirname(here), "waveforminversionust_b200", "mex")
+    for name in ("decompBlockLU.c", "applyBlockLU.c"):
+        subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(here, "mex_stub"),
+                        "-I", os.path.dirname(HEADER), os.path.join(mex_dir, name)], check=True)

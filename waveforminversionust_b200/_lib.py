@@ -30,7 +30,7 @@ EXPORTED = (
     "wust_decomp_block_lu", "wust_decomp_block_lu_noalloc", "wust_apply_block_lu",
     "wust_solver_create", "wust_solver_refactor", "wust_solver_destroy", "wust_solver_timings",
     "wust_solver_stencil", "wust_solver_block", "wust_solver_solve", "wust_solver_mass_apply",
-    "wust_solver_oracle", "wust_solver_curvature", "wust_solver_stats", "wust_solver_factor_stats",
+    "wust_solver_oracle", "wust_solver_curvature", "wust_solver_stats", "wust_solver_factor_stats", "wust_solver_sweep_times",
     "wust_selftest_barrier_timeout",
 )
 
@@ -53,7 +53,7 @@ class SolverOptions(C.Structure):
         ("stencil_vmin", C.c_double), ("stencil_vmax", C.c_double),
         ("dispersion", C.c_int), ("time_step_s", C.c_double), ("reference_speed_mps", C.c_double),
         ("precision", C.c_int), ("refine_max_iters", C.c_int), ("refine_tol", C.c_double),
-        ("max_sources", C.c_int),
+        ("max_sources", C.c_int), ("factor_method", C.c_int),
     ]
 
 
@@ -89,6 +89,7 @@ def load() -> C.CDLL:
     lib.wust_solver_curvature.argtypes = [vp, vp, pd]
     lib.wust_solver_stats.argtypes = [vp, pi, pd, pd, C.POINTER(C.c_longlong)]
     lib.wust_solver_factor_stats.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.wust_solver_sweep_times.argtypes = [vp, pd, C.POINTER(C.c_longlong)]
     lib.wust_selftest_barrier_timeout.argtypes = [i, pi]
     for name in EXPORTED:
         if name not in ("wust_status_id", "wust_last_error"):

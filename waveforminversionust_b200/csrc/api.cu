@@ -92,6 +92,7 @@ using namespace wust;
 struct wust_solver {
     int ny = 0, nx = 0, smax = 0, precision = 0, refine_max = 8;
     double refine_tol = 1e-5;
+    int factor_method = WUST_FACTOR_DEFAULT;
     double f = 0, sgn = -1, a0 = 0, L = 0, vmin = 0, vmax = 0;
     int ldr9 = 0;
     double dt = 0, cr = 0;
@@ -149,6 +150,10 @@ struct wust_solver {
     double last_error_est = 0;
     long long launches = 0;
     cudaEvent_t ev[4] = {};
+    // device time of every block-LU sweep pair (forward + backward) since creation
+    cudaEvent_t sw_ev[2] = {};
+    double sweep_ms = 0;
+    long long sweeps = 0;
 
     Coefs<float2> coefs64() const {
         Coefs<float2> c;
@@ -187,6 +192,7 @@ static void free_solver(wust_solver *s) {
     for (void *p : ptrs) dfree(p);
     for (int i = 0; i < 9; ++i) { dfree(s->c128[i]); dfree(s->c64[i]); }
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
+    for (auto &e : s->sw_ev) if (e) cudaEventDestroy(e);
     delete s;
 }
 
@@ -302,12 +308,19 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
 // One sweep pair (forward+backward) with the profile's arithmetic: CUDA-core
 // complex single, or tcgen05 TF32 GEMMs on the packed invT operands.
 static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
+    WUST_CUDA(cudaEventRecord(s->sw_ev[0], s->st));
     if (s->precision == WUST_PRECISION_TF32_REFINED) {
         tc_sweep_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->tc_geom, src, S, adjoint, out, s->tc_b,
                        s->tc_part, s->tc_sync, s->tc_err, s->st);
     } else {
         sweep_solve(s->coefs64(), s->invT, src, S, adjoint, out, s->tmp, s->st);
     }
+    WUST_CUDA(cudaEventRecord(s->sw_ev[1], s->st));
+    WUST_CUDA(cudaEventSynchronize(s->sw_ev[1]));
+    float ms = 0;
+    WUST_CUDA(cudaEventElapsedTime(&ms, s->sw_ev[0], s->sw_ev[1]));
+    s->sweep_ms += ms;
+    ++s->sweeps;
 }
 
 static void check_tc_err(wust_solver *s) {
@@ -511,6 +524,9 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         s = new wust_solver();
         s->ny = o->ny; s->nx = o->nx;
         s->smax = o->max_sources > 0 ? o->max_sources : 256;
+        if (o->factor_method < WUST_FACTOR_DEFAULT || o->factor_method > WUST_FACTOR_GAUSS_JORDAN)
+            fail(WUST_ERR_INVALID_INPUT, "unknown factor_method %d", o->factor_method);
+        s->factor_method = o->factor_method;
         s->precision = o->precision;
         s->refine_max = o->refine_max_iters > 0 ? o->refine_max_iters : 8;
         s->refine_tol = o->refine_tol > 0 ? o->refine_tol : 1e-5;
@@ -538,6 +554,7 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         WUST_CUDA(cudaGetDevice(&s->device));
         s->st = (cudaStream_t)stream;
         for (auto &e : s->ev) WUST_CUDA(cudaEventCreate(&e));
+        for (auto &e : s->sw_ev) WUST_CUDA(cudaEventCreate(&e));
         const size_t N = s->plane();
         const int ny = s->ny, nx = s->nx;
         s->vel = dalloc<double>(N);
@@ -576,8 +593,10 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
             s->tc_b = dalloc<uint8_t>(s->tc_geom.b_bytes);
             s->tc_part = dalloc<float>(s->tc_geom.part_bytes / sizeof(float));
             s->tc_sync = dalloc<unsigned>(s->tc_geom.sync_words);
-            s->ns_g = ns_geom(ny, ns_max_ctas());
-            if (s->ns_g.ks > 0) WUST_CUDA(cudaMalloc(&s->ns_scratch, s->ns_g.scratch_bytes));
+            if (s->factor_method == WUST_FACTOR_DEFAULT) {
+                s->ns_g = ns_geom(ny, ns_max_ctas());
+                if (s->ns_g.ks > 0) WUST_CUDA(cudaMalloc(&s->ns_scratch, s->ns_g.scratch_bytes));
+            }
             s->tc_err = dalloc<int>(4);
             WUST_CUDA(cudaMemset(s->tc_err, 0, 4 * sizeof(int)));
         }
@@ -823,6 +842,14 @@ int wust_solver_stats(const wust_solver *s, int *refine_iters, double *final_res
         if (final_residual) *final_residual = s->last_residual;
         if (error_estimate) *error_estimate = s->last_error_est;
         if (kernel_launches) *kernel_launches = s->launches;
+    });
+}
+
+int wust_solver_sweep_times(const wust_solver *s, double *total_ms, long long *count) {
+    return guarded([&] {
+        if (!s) fail(WUST_ERR_INVALID_INPUT, "null solver");
+        if (total_ms) *total_ms = s->sweep_ms;
+        if (count) *count = s->sweeps;
     });
 }
 

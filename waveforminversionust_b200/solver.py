@@ -60,7 +60,8 @@ class HelmholtzSolver:
 
     def __init__(self, x, y, vel, atten, f, signConvention, a0, L_PML, options, *,
                  precision: str = "c64", refine_tol: float = 1e-5, refine_max_iters: int = 8,
-                 max_sources: int | None = None, stream: torch.cuda.Stream | None = None):
+                 max_sources: int | None = None, stream: torch.cuda.Stream | None = None,
+                 factor_method: str = "default"):
         if not isinstance(options, dict) or "backend" not in options or "stencil_bounds" not in options:
             raise WustError(1, "Explicit backend and fixed stencil_bounds are required")
         bounds = options["stencil_bounds"]
@@ -98,6 +99,10 @@ class HelmholtzSolver:
         opts.precision = _lib.PRECISION[precision]
         opts.refine_max_iters = int(refine_max_iters)
         opts.refine_tol = float(refine_tol)
+        methods = {"default": 0, "gauss-jordan": 1}
+        if factor_method not in methods:
+            raise WustError(1, f"factor_method must be one of {sorted(methods)}")
+        opts.factor_method = methods[factor_method]
         opts.max_sources = int(max_sources or 256)
         self._opts = opts
         self.precision = precision
@@ -215,6 +220,12 @@ class HelmholtzSolver:
         check(self._lib.wust_solver_stats(self._h, C.byref(it), C.byref(res), C.byref(err), C.byref(nl)))
         return {"refine_iters": it.value, "final_residual": res.value, "error_estimate": err.value,
                 "kernel_launches": nl.value}
+
+    def sweep_times(self):
+        """Total device milliseconds and count of the sweep pairs run so far."""
+        ms, n = C.c_double(), C.c_longlong()
+        check(self._lib.wust_solver_sweep_times(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def factor_stats(self):
         """How the last factorization inverted its Schur pages."""
