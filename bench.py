@@ -38,6 +38,10 @@ WORKLOADS = {
     "config2": dict(n_tx=256, freq=1.2e6,
                     text="config2 gradient: 552x552 grid (512^2 + 20-cell PML), dx 0.25 mm, 256 TX x 256 RX ring "
                          "r = 55 mm, f = 1.2 MHz, breast-like phantom"),
+    # mid-size case for ncu captures of the tensor-core kernels (same launch
+    # shapes as 552^2 with 256 sources: 112-144 CTAs; a few GB on the device)
+    "mid400": dict(n_tx=256, freq=0.9e6,
+                   text="mid400: 400x400 grid (368^2 + 16-cell PML), dx 0.3 mm, 256 TX x 256 RX ring, f = 0.9 MHz"),
     # seconds-scale case used for ncu captures of the same kernels
     "config1": dict(n_tx=32, freq=0.5e6,
                     text="config1 gradient: 224x224 grid (192^2 + 16-cell PML), dx 0.4 mm, 32 TX x 128 RX ring "
@@ -111,6 +115,8 @@ def make_problem(seed: int = 0):
     from waveforminversionust_b200 import synthetic
     if WORKLOAD == "config1":
         return synthetic.config1(seed=seed)
+    if WORKLOAD == "mid400":
+        return synthetic.small(seed=seed, n_interior=368, pml=16, dx=0.3e-3, n_elem=256, n_tx=256, freqs=(FREQ,))
     return synthetic.config2(seed=seed, freqs=[FREQ])
 
 
