@@ -369,7 +369,7 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
                  s->refine_tol, s->refine_max, s->last_error_est);
         rn_prev = rn;
         run_sweep(s, dense, S, adjoint, s->d32);
-        accumulate_launch(s->d32, s->x64, plane, S, s->dnorm2, s->xnorm2, st);
+        accumulate_launch(s->d32, s->x64, s->ny, s->nx, S, s->dnorm2, s->xnorm2, st);
         residual_launch(s->coefs128(), src, s->x64, S, adjoint, s->r32, s->rnorm2, nullptr, st);
         WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaMemcpyAsync(dn.data(), s->dnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -124,7 +124,7 @@ void residual_launch(const Coefs<double2> &co, const SrcView &b, const double2 *
                      float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st);
 void promote_launch(const float2 *u, double2 *x, size_t n, cudaStream_t st);          // x = u
 // x += d per source plane; per-source squared norms of d and of the new x
-void accumulate_launch(const float2 *d, double2 *x, size_t plane, int S, double *dnorm2, double *xnorm2,
+void accumulate_launch(const float2 *d, double2 *x, int ny, int nx, int S, double *dnorm2, double *xnorm2,
                        cudaStream_t st);
 void demote_launch(const double2 *x, float2 *u, size_t n, cudaStream_t st);           // u = x
 

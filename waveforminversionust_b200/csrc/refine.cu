@@ -5,7 +5,11 @@
 // (HelmholtzSolver.m:118-135) and its conjugate transpose.  Rows on the top
 // and bottom Dirichlet border (y = 0, Ny-1) are excluded: the block solver
 // keeps them at zero (applyBlockLU.cu:10), so they never enter the other
-// equations and cannot be corrected.
+// equations and cannot be corrected.  The norms that steer the refinement
+// (residual, correction, solution) are taken over the interior grid only:
+// the whole Dirichlet ring is zero in forward fields and is zeroed by M^T
+// before an adjoint field is used, while the block adjoint leaves its own
+// values there that a correction cannot settle.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -77,8 +81,10 @@ __global__ void __launch_bounds__(kResThreads) residual_kernel(Coefs<double2> co
                 }
                 const double2 bv = z_from(b.get(y, xi, s, ny, nx));
                 r = zsub(bv, h);
-                rr = zabs2(r);
-                bb = zabs2(bv);
+                if (xi > 0 && xi < nx - 1) {        // norms over the interior grid (see accumulate_kernel)
+                    rr = zabs2(r);
+                    bb = zabs2(bv);
+                }
             }
             r32[plane * s + me] = c_from(r);
         }
@@ -116,8 +122,13 @@ __global__ void promote_kernel(const float2 *u, double2 *x, size_t n) {
         x[i] = z_from(u[i]);
 }
 // x += d over one source plane per blockIdx.y; per-source ||d||^2 and ||x||^2.
-__global__ void accumulate_kernel(const float2 *d, double2 *x, size_t plane, double *dnorm2, double *xnorm2) {
+// Norms over the interior grid: the Dirichlet ring (rows 0, ny-1, columns 0,
+// nx-1) is zero in forward fields and is zeroed by M^T before an adjoint
+// field is used (HelmholtzSolver.m:211-219), so its values do not enter any
+// result and do not decide when a refinement has converged.
+__global__ void accumulate_kernel(const float2 *d, double2 *x, int ny, int nx, double *dnorm2, double *xnorm2) {
     const int s = blockIdx.y;
+    const size_t plane = (size_t)ny * nx;
     const float2 *ds = d + plane * s;
     double2 *xs = x + plane * s;
     double dd = 0, xx = 0;
@@ -126,8 +137,11 @@ __global__ void accumulate_kernel(const float2 *d, double2 *x, size_t plane, dou
         const float2 b = ds[i];
         const double2 v = make_double2(a.x + (double)b.x, a.y + (double)b.y);
         xs[i] = v;
-        dd += (double)b.x * b.x + (double)b.y * b.y;
-        xx += v.x * v.x + v.y * v.y;
+        const int y = (int)(i % ny), xc = (int)(i / ny);
+        if (y > 0 && y < ny - 1 && xc > 0 && xc < nx - 1) {
+            dd += (double)b.x * b.x + (double)b.y * b.y;
+            xx += v.x * v.x + v.y * v.y;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -151,12 +165,13 @@ void promote_launch(const float2 *u, double2 *x, size_t n, cudaStream_t st) {
     ++g_kernel_launches;
     WUST_LAUNCH_CHECK();
 }
-void accumulate_launch(const float2 *d, double2 *x, size_t plane, int S, double *dnorm2, double *xnorm2,
+void accumulate_launch(const float2 *d, double2 *x, int ny, int nx, int S, double *dnorm2, double *xnorm2,
                        cudaStream_t st) {
+    const size_t plane = (size_t)ny * nx;
     WUST_CUDA(cudaMemsetAsync(dnorm2, 0, sizeof(double) * S, st));
     WUST_CUDA(cudaMemsetAsync(xnorm2, 0, sizeof(double) * S, st));
     dim3 grid((unsigned)std::min<size_t>((plane + 255) / 256, 64), S);
-    accumulate_kernel<<<grid, 256, 0, st>>>(d, x, plane, dnorm2, xnorm2);
+    accumulate_kernel<<<grid, 256, 0, st>>>(d, x, ny, nx, dnorm2, xnorm2);
     ++g_kernel_launches;
     WUST_LAUNCH_CHECK();
 }
