@@ -111,6 +111,23 @@ class ClockSampler:
                     samples=len(sm))
 
 
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """Max of a per-rank time over the process group (identity on one rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, steps: int, max_ms: float) -> float:
+    """Whole-job gradients/s: every rank runs `steps` gradients (replicas),
+    timed by the slowest rank."""
+    return world * steps / (max_ms * 1e-3)
+
+
 def make_problem(seed: int = 0):
     from waveforminversionust_b200 import synthetic
     if WORKLOAD == "config1":
@@ -267,12 +284,6 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     def measure(precision: str, with_e2e: bool):
         cfg = default_config(pml_m=p.pml_m, precision=precision, source_batch_size=N_TX)
@@ -324,10 +335,10 @@ def main():
                 launches += solver.stats()["kernel_launches"] + 1
             ev1.record(stream)
             barrier()
-        dev_ms = max_over_ranks(ev0.elapsed_time(ev1))
+        dev_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
         sw_ms1, sw_n1 = solver.sweep_times()
         stats = solver.stats()
-        res = dict(ms_per_step=dev_ms / args.steps, value=world * args.steps / (dev_ms * 1e-3),
+        res = dict(ms_per_step=dev_ms / args.steps, value=aggregate_rate(world, args.steps, dev_ms),
                    factor_ms=float(np.mean(fac_ms)), launches_per_step=launches / args.steps,
                    refine_iters=stats["refine_iters"], final_residual=stats["final_residual"],
                    loss=loss.value, clocks=clk.summary(),
@@ -343,11 +354,11 @@ def main():
                 step_host()
             ev1.record(stream)
             barrier()
-            e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+            e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
             N = ny * nx
             h2d = N * 8 + 4 * (obs.n_tx + obs.n_rx) + obs.n_tx * obs.n_rx * (8 + 1) + N * 4
             d2h = N * 8 + obs.n_tx * 8
-            res["e2e"] = dict(value=world * args.steps / (e2e_ms * 1e-3), unit="gradients/s",
+            res["e2e"] = dict(value=aggregate_rate(world, args.steps, e2e_ms), unit="gradients/s",
                               h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                               wall_ms_per_step=(time.perf_counter() - t0) * 1e3 / args.steps)
         solver.close()

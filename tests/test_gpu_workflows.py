@@ -1,0 +1,85 @@
+"""GPU tests of the library's callers: the autograd misfit, the k-Wave LDR-9
+dispersion option and the NCG reconstruction loop, each against the FP64
+oracle or its defining property (calls go through the C ABI)."""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+
+
+def _gpu_obs(o_obs):
+    from waveforminversionust_b200.objective import Observations
+    return Observations(o_obs.x_m, o_obs.y_m, o_obs.tx_index, o_obs.rx_index, o_obs.frequencies_hz, o_obs.Y,
+                        o_obs.mask)
+
+
+@pytest.mark.parametrize("precision", ["c64-refined", "tf32-refined"])
+def test_autograd_misfit_matches_central_differences(ref_fixture, precision):
+    """torch.autograd over Phi_f(s): backward (adjoint solve + slowness
+    gradient, factors reused) against central differences at relative steps
+    1e-3 .. 1e-5, FP64 tolerance 1e-4 (test_runtime.m:45-56)."""
+    import torch
+    from waveforminversionust_b200.autograd import misfit
+    from waveforminversionust_b200.objective import POOL, default_config
+    fx = ref_fixture
+    obs = _gpu_obs(fx["obs"])
+    cfg = default_config(pml_m=.004, pml_strength=10, source_batch_size=2, precision=precision, refine_tol=1e-10)
+    s0 = torch.tensor(1 / fx["initial"], dtype=torch.float64, device="cuda", requires_grad=True)
+    loss = misfit(s0, obs, 0, cfg)
+    loss.backward()
+    d = torch.tensor(fx["direction"], dtype=torch.float64, device="cuda")
+    adj = float((s0.grad * d).sum())
+    for rel_step in (1e-3, 1e-4, 1e-5):
+        h = rel_step * float(s0.detach().abs().max()) / float(d.abs().max())
+        with torch.no_grad():
+            lp = float(misfit(s0.detach() + h * d, obs, 0, cfg))
+            lm = float(misfit(s0.detach() - h * d, obs, 0, cfg))
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - adj) / max(abs(fd), abs(adj)) < 1e-4, (rel_step, fd, adj)
+    POOL.clear()
+
+
+def test_ldr9_dispersion_matches_oracle(ref_fixture):
+    """wavenumber='kwave-ldr9' (kwaveLdr9WavenumberSquared.m) on the GPU: the
+    refined misfit and gradient equal the FP64 oracle's."""
+    from oracle import helmholtz_fp64 as o
+    from waveforminversionust_b200.objective import POOL, default_config, wust_oracle
+    fx = ref_fixture
+    disp = dict(time_step_s=2e-8, reference_speed_mps=1700)
+    cfg_o = o.OracleConfig(pml_m=.004, source_batch_size=2, wavenumber="kwave-ldr9", dispersion=disp)
+    loss_ref, grad_ref, _ = o.wust_oracle(fx["initial"], fx["obs"], 0, cfg_o)
+    cfg = default_config(pml_m=.004, pml_strength=10, source_batch_size=2, precision="c64-refined", refine_tol=1e-10,
+                         wavenumber="kwave-ldr9", dispersion=disp)
+    loss, grad = wust_oracle(fx["initial"], _gpu_obs(fx["obs"]), 0, cfg)
+    assert abs(loss - loss_ref) / loss_ref < 1e-7
+    assert np.linalg.norm(grad - grad_ref) / np.linalg.norm(grad_ref) < 1e-5
+    # the dispersion option changes the operator (it is not silently ignored)
+    loss_cont, _ = wust_oracle(fx["initial"], _gpu_obs(fx["obs"]), 0,
+                               default_config(pml_m=.004, pml_strength=10, source_batch_size=2,
+                                              precision="c64-refined", refine_tol=1e-10))
+    assert abs(loss_cont - loss) / loss > 1e-6
+    POOL.clear()
+
+
+def test_reconstruction_descends_and_matches_oracle_first_step(ref_fixture):
+    """Three NCG updates of wust_reconstruct (wust_reconstruct.m:20-74) at one
+    frequency on the GPU: the misfit before each update decreases, and the
+    first misfit equals the FP64 oracle's."""
+    from oracle import helmholtz_fp64 as o
+    from waveforminversionust_b200.objective import POOL
+    from waveforminversionust_b200.reconstruct import wust_reconstruct
+    fx = ref_fixture
+    obs = _gpu_obs(fx["obs"])
+    cfg = dict(backend="gpu", bounds_mps=(1300.0, 1800.0), max_update_mps=12.0, step_damping=1.0,
+               source_batch_size=2, pml_strength=10.0, pml_m=.004, stencil_bounds=(1400.0, 1700.0),
+               wavenumber="continuum", filter_cutoff=0.0, filter_order=4, update_mask=fx["mask"].astype(float),
+               frequency_schedule_hz=[1e5, 1e5, 1e5], precision="c64-refined")
+    out = wust_reconstruct(obs, fx["initial"], cfg)
+    losses = [r["loss_before_update"] for r in out["records"]]
+    assert len(losses) == 3 and losses[1] < losses[0] and losses[2] < losses[1], losses
+    loss0, _, _ = o.wust_oracle(fx["initial"], fx["obs"], 0, fx["cfg"], need_gradient=False)
+    assert abs(losses[0] - loss0) / loss0 < 1e-5
+    assert all(r["curvature"] > 0 and r["alpha"] >= 0 for r in out["records"])
+    POOL.clear()
