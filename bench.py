@@ -392,8 +392,16 @@ def main():
         achieved = flop / (head["factor_ms"] * 1e-3) / 1e12
         kname = ("ns_factor_kernel + factor_kernel (Newton-Schulz Schur inverses, Gauss-Jordan pages)"
                  if args.precision == "tf32-refined" else "factor_kernel (Schur recursion + Gauss-Jordan inverses)")
+    # DRAM bytes of one launch of the dominant kernel, measured with ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on this kernel
+    # at 552^2 with 256 sources: 6.91 GB read + 1.22 GB written per sweep pair
+    traffic = None
+    if flop == fl["apply"] and args.precision == "tf32-refined" and WORKLOAD == "config2":
+        traffic = 8.13e9
     roofline = dict(kernel=kname, bound="tensor", achieved=achieved, peak=peak_tf, unit="TFLOP/s",
-                    frac=achieved / peak_tf, peak_source=peak_src, traffic=None,
+                    frac=achieved / peak_tf, peak_source=peak_src, traffic=traffic,
+                    traffic_unit="bytes per launch (ncu)", hbm_gbs_achieved=(
+                        traffic / (head["sweep_ms_per_launch"] * 1e-3) / 1e9 if traffic else None),
                     algorithmic_flop_per_launch=flop,
                     launch_ms=head["sweep_ms_per_launch"] if flop == fl["apply"] else head["factor_ms"])
     cpu = None
