@@ -76,58 +76,11 @@ __host__ __device__ __forceinline__ double2 z_from(float2 a) { return make_doubl
 __host__ __device__ __forceinline__ float2 c_from(double2 a) { return make_float2((float)a.x, (float)a.y); }
 __host__ __device__ __forceinline__ double zabs2(double2 a) { return a.x * a.x + a.y * a.y; }
 
-// ---------------------------------------------------------------------------
-// Bounded device-wide barrier for persistent cooperative kernels.  Every wait
-// is capped by a wall-clock budget read from %globaltimer; on expiry the
-// kernel records the barrier site in `error` and all CTAs return.
-// ---------------------------------------------------------------------------
-struct GridBarrier {
-    unsigned int count;
-    unsigned int generation;
-    int error;      // 0 = ok, otherwise the site id of the first expired wait
-    int pad;
-};
-
+// %globaltimer in nanoseconds: the clock of every bounded device-side wait.
 __device__ __forceinline__ unsigned long long global_timer_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
-}
-
-// Returns false when the barrier failed (timeout here or elsewhere).
-__device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned int nblocks,
-                                          unsigned long long timeout_ns, int site) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        volatile unsigned int *vgen = &bar->generation;
-        volatile int *verr = &bar->error;
-        unsigned int gen = *vgen;
-        __threadfence();
-        unsigned int arrived = atomicAdd(&bar->count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&bar->count, 0u);
-            __threadfence();
-            atomicAdd(&bar->generation, 1u);
-        } else {
-            unsigned long long t0 = global_timer_ns();
-            while (*vgen == gen) {
-                if (*verr != 0) { ok = 0; break; }
-                if (global_timer_ns() - t0 > timeout_ns) {
-                    atomicCAS(&bar->error, 0, site);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        if (*verr != 0) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
 }
 
 // ---------------------------------------------------------------------------

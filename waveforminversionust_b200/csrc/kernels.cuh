@@ -5,8 +5,6 @@
 
 namespace wust {
 
-enum SweepMode { SWEEP_F1 = 0, SWEEP_F2 = 1, SWEEP_A1 = 2, SWEEP_A2 = 3 };
-
 // ---- factor.cu -------------------------------------------------------------
 constexpr int kFactorTile = 48;
 // padded interior size of a working page (multiple of the output tile)

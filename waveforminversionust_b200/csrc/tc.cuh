@@ -12,10 +12,9 @@
 //         (row-group direction) 1024 B.
 //   One MMA consumes 32 bytes of K (bf16: K = 16, tf32: K = 8), i.e. two
 //   core matrices, so the descriptor start advances 256 B per MMA.
-// The K loop runs through a STAGES-deep shared-memory ring: a single thread
-// issues the bulk copies (mbarrier complete_tx), the MMAs (accumulating in
-// TMEM) and tcgen05.commit arrivals that free a stage once its MMAs retired.
-// Every wait is bounded by a %globaltimer budget and reports failure.
+// A single thread issues the bulk copies (mbarrier complete_tx), the MMAs
+// (accumulating in TMEM) and the tcgen05.commit arrivals; every wait is
+// bounded by a %globaltimer budget and reports failure.
 #pragma once
 
 #include <stdint.h>
@@ -140,78 +139,6 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]);
-}
-
-// Shared-memory footprint of a STAGES-deep ring for TN-row B tiles.
-template <int TN, int STAGES>
-struct Ring {
-    static constexpr int kBChunk = TN * kChunkBytes;
-    static constexpr int kBytes = STAGES * (kAChunk + kBChunk) + (2 * STAGES + 2) * 8 + 16;
-};
-
-// Single-thread K loop: D(tmem) = A * B^T over nchunks chunks.
-// A chunk c at a_base + c * a_stride, B chunk c at b_base + c * b_stride.
-// Returns false on a timed-out wait; always commits `done` at the end so the
-// epilogue can wait on it (phase = done_phase).
-template <bool TF32, int TN, int STAGES>
-__device__ bool tile_mainloop(uint8_t *sA, uint8_t *sB, uint64_t *full, uint64_t *empty, uint64_t *done,
-                              uint32_t (&full_phase)[STAGES], uint32_t (&empty_phase)[STAGES],
-                              const uint8_t *a_base, size_t a_stride, const uint8_t *b_base, size_t b_stride,
-                              int nchunks, uint32_t tmem, unsigned long long timeout_ns) {
-    constexpr int kB = TN * kChunkBytes;
-    constexpr uint32_t kIdesc = instr_desc<TF32>(kTileRows, TN);
-    bool ok = true;
-    int issued = 0;      // chunks whose copies were issued
-    int consumed = 0;    // chunks whose full barrier was waited
-    for (int c = 0; c < STAGES - 1 && c < nchunks; ++c) {
-        mbar_expect_tx(&full[c], kAChunk + kB);
-        bulk_g2s(sA + c * kAChunk, a_base + c * a_stride, kAChunk, &full[c]);
-        bulk_g2s(sB + c * kB, b_base + c * b_stride, kB, &full[c]);
-        ++issued;
-    }
-    for (int c = 0; c < nchunks; ++c) {
-        const int s = c % STAGES;
-        if (!mbar_wait(&full[s], full_phase[s], timeout_ns)) { ok = false; break; }
-        full_phase[s] ^= 1u;
-        ++consumed;
-        fence_after();
-#pragma unroll
-        for (int k = 0; k < kChunkBytes / 32; ++k)
-            mma<TF32>(tmem, smem_desc(sA + s * kAChunk + k * 256), smem_desc(sB + s * kB + k * 256), kIdesc,
-                      (c > 0 || k > 0) ? 1u : 0u);
-        commit(&empty[s]);
-        const int nc = c + STAGES - 1;
-        if (nc < nchunks) {
-            // stage nc % STAGES last held chunk c - 1: wait for its MMAs to retire
-            const int s2 = nc % STAGES;
-            if (c >= 1) {
-                if (!mbar_wait(&empty[s2], empty_phase[s2], timeout_ns)) { ok = false; break; }
-                empty_phase[s2] ^= 1u;
-            }
-            mbar_expect_tx(&full[s2], kAChunk + kB);
-            bulk_g2s(sA + s2 * kAChunk, a_base + nc * a_stride, kAChunk, &full[s2]);
-            bulk_g2s(sB + s2 * kB, b_base + nc * b_stride, kB, &full[s2]);
-            ++issued;
-        }
-    }
-    if (ok) {
-        // Chunks [max(0, nchunks - STAGES), nchunks) were committed but never
-        // waited; retire them so every stage's phase stays in step for the
-        // next tile that reuses the ring.
-        for (int c = (nchunks > STAGES ? nchunks - STAGES : 0); c < nchunks; ++c) {
-            const int s = c % STAGES;
-            if (!mbar_wait(&empty[s], empty_phase[s], timeout_ns)) { ok = false; break; }
-            empty_phase[s] ^= 1u;
-        }
-    } else {
-        // Let copies already in flight land before the CTA gives up (bounded).
-        for (int c = consumed; c < issued; ++c) {
-            const int s = c % STAGES;
-            if (mbar_wait(&full[s], full_phase[s], timeout_ns)) full_phase[s] ^= 1u;
-        }
-    }
-    commit(done);
-    return ok;
 }
 
 }  // namespace tc
