@@ -83,3 +83,48 @@ def test_reconstruction_descends_and_matches_oracle_first_step(ref_fixture):
     assert abs(losses[0] - loss0) / loss0 < 1e-5
     assert all(r["curvature"] > 0 and r["alpha"] >= 0 for r in out["records"])
     POOL.clear()
+
+
+@pytest.fixture(scope="module")
+def small():
+    from waveforminversionust_b200 import synthetic
+    return synthetic.small(seed=3), None
+
+
+def test_tensor_core_profile_edge_cases(small):
+    """TF32 profile: an all-zero right-hand side returns zeros, a single
+    source agrees with the c64 refined profile, more sources than one call
+    holds are batched, and grids beyond the tensor-core tiling are rejected
+    with WUST:InvalidInput."""
+    from waveforminversionust_b200._lib import WustError
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    p, ref = small
+    ny, nx = p.shape
+    opts = dict(backend="gpu", stencil_bounds=(1400, 1700))
+    f = p.frequencies_hz[0]
+    tc = HelmholtzSolver(p.x_m, p.y_m, p.c_true, None, f, -1, 10.0, p.pml_m, opts, precision="tf32-refined",
+                         max_sources=4)
+    z = tc.solve(np.zeros((ny, nx, 3), np.complex64)).cpu().numpy()
+    assert np.all(z == 0)
+    rng = np.random.default_rng(2)
+    b = np.zeros((ny, nx, 1), np.complex64)
+    b[1:-1, 1:-1, 0] = rng.standard_normal((ny - 2, nx - 2)) + 1j * rng.standard_normal((ny - 2, nx - 2))
+    c64 = HelmholtzSolver(p.x_m, p.y_m, p.c_true, None, f, -1, 10.0, p.pml_m, opts, precision="c64-refined",
+                          max_sources=4)
+    for adjoint in (False, True):
+        a = tc.solve(b, adjoint=adjoint).cpu().numpy()[1:-1, 1:-1]
+        w = c64.solve(b, adjoint=adjoint).cpu().numpy()[1:-1, 1:-1]
+        assert np.linalg.norm(a - w) / np.linalg.norm(w) < 3e-5, adjoint
+    # more sources than one call holds: the Python solver batches them
+    b5 = np.repeat(b, 5, axis=2)
+    u5 = tc.solve(b5).cpu().numpy()
+    u1 = tc.solve(b).cpu().numpy()
+    assert np.linalg.norm(u5 - u1) / np.linalg.norm(u1) < 1e-6
+    tc.close()
+    c64.close()
+    n = 600                                   # beyond the 4 x 9 x 16-row tensor-core K tiling
+    xg = (np.arange(n) - (n - 1) / 2) * 3e-4
+    with pytest.raises(WustError) as e:
+        HelmholtzSolver(xg, xg, np.full((n, n), 1500.0), None, 5e5, -1, 10.0, 16 * 3e-4, opts,
+                        precision="tf32-refined", max_sources=4)
+    assert e.value.identifier == "WUST:InvalidInput"
