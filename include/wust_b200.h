@@ -142,6 +142,7 @@ typedef struct {
     double refine_tol;             /* refined profiles: relative FP64 residual target (0 -> 1e-5) */
     int max_sources;               /* largest RHS batch the object will see (0 -> 256) */
     int factor_method;             /* WUST_FACTOR_*: how the Schur pages are inverted */
+    int sweep_method;              /* WUST_SWEEP_*: how the TF32 profile runs its sweeps */
 } wust_solver_options;
 
 /* Schur-page inversion (no counterpart in the reference, which always uses
@@ -149,6 +150,13 @@ typedef struct {
  * profile, Gauss-Jordan otherwise; GAUSS_JORDAN: complex-single Gauss-Jordan
  * for every profile (the TF32 profile then keeps tensor-core sweeps only). */
 enum wust_factor_method { WUST_FACTOR_DEFAULT = 0, WUST_FACTOR_GAUSS_JORDAN = 1 };
+
+/* Sweeps of the TF32 profile (no counterpart in the reference, whose
+ * applyBlockLU runs the columns one after the other).  DEFAULT: column
+ * chunks solved concurrently and joined by their composed propagators
+ * (formed once per factorization); SEQUENTIAL: one column step after the
+ * other on all SMs.  Both apply the same block-LU operator. */
+enum wust_sweep_method { WUST_SWEEP_DEFAULT = 0, WUST_SWEEP_SEQUENTIAL = 1 };
 
 /* Assemble the nine-point PML operator on the GPU and factorize it.
  * vel, atten: ny x nx (atten may be NULL = zero).  stream may be NULL. */

@@ -163,6 +163,40 @@ def test_tensor_core_sweep_split_k_and_source_batches():
         assert rel(a, b) < 1e-7, adjoint
 
 
+@pytest.mark.parametrize("ny,nx,S,pml_cells", [(300, 340, 300, 16), (130, 9, 20, 3)])
+def test_chunked_sweeps_match_sequential(ny, nx, S, pml_cells):
+    """The column-chunked TF32 sweeps (chunks solved concurrently, joined by
+    their composed propagators) apply the same block-LU operator as the
+    sequential TF32 sweeps: refined to 1e-9 both give the same fields, and
+    the chunked sweep needs at most one correction more.  Grids: 26 chunks
+    with two source tiles (256 + 44), and 4 chunks on a narrow grid."""
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    dx = 0.3e-3
+    x = (np.arange(nx) - (nx - 1) / 2) * dx
+    y = (np.arange(ny) - (ny - 1) / 2) * dx
+    X, Y = np.meshgrid(x, y)
+    c = 1500 + 40 * np.exp(-((X - 2e-3) ** 2 + Y ** 2) / (2 * (8e-3) ** 2))
+    sols, iters = {}, {}
+    for method in ("default", "sequential"):
+        s = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, pml_cells * dx,
+                            dict(backend="gpu", stencil_bounds=(1400, 1700)), precision="tf32-refined",
+                            refine_tol=1e-9, max_sources=S, sweep_method=method)
+        for adjoint in (False, True):
+            r = np.zeros((ny, nx, S), np.complex64)
+            g = np.random.default_rng(5 + adjoint)
+            r[1:-1, 1:-1] = g.standard_normal((ny - 2, nx - 2, S)) + 1j * g.standard_normal((ny - 2, nx - 2, S))
+            sols[method, adjoint] = to_np(s.solve(r, adjoint=adjoint))
+            st = s.stats()
+            assert st["error_estimate"] <= 1e-9, (method, adjoint, st)
+            iters[method, adjoint] = st["refine_iters"]
+        s.close()
+    for adjoint in (False, True):
+        a = sols["default", adjoint][1:-1, 1:-1]
+        b = sols["sequential", adjoint][1:-1, 1:-1]
+        assert rel(a, b) < 1e-7, adjoint
+        assert iters["default", adjoint] <= iters["sequential", adjoint] + 1, iters
+
+
 def test_newton_schulz_factor_agrees_with_gauss_jordan():
     """The TF32 profile's Schur inverses (Newton-Schulz iterations on the
     tensor cores, Gauss-Jordan on the pages where the previous inverse is no
@@ -298,7 +332,10 @@ def test_config1_gradient_parity():
     o_obs = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, p.frequencies_hz, Yobs, np.ones((32, 128, 1), bool))
     loss_ref, grad_ref, _ = o.wust_oracle(p.c_init, o_obs, 0, cfg_o)
     obs = Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, p.frequencies_hz, Yobs, np.ones((32, 128, 1), bool))
-    for precision, tl, tg in (("c64", 1e-3, 1e-2), ("c64-refined", 1e-6, 1e-4), ("tf32-refined", 1e-6, 1e-4)):
+    # Refined profiles stop at an estimated forward error of 1e-5 (the pressure
+    # tolerance); the TF32 sweeps contract less per correction than the
+    # complex-single ones, so their misfit is held to that 1e-5 bound.
+    for precision, tl, tg in (("c64", 1e-3, 1e-2), ("c64-refined", 1e-6, 1e-4), ("tf32-refined", 1e-5, 1e-4)):
         loss, grad = wust_oracle(p.c_init, obs, 0, default_config(pml_m=p.pml_m, precision=precision))
         assert abs(loss - loss_ref) / loss_ref < tl, precision
         assert rel(grad, grad_ref) < tg, precision

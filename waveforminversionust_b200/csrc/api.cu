@@ -93,6 +93,7 @@ struct wust_solver {
     int ny = 0, nx = 0, smax = 0, precision = 0, refine_max = 8;
     double refine_tol = 1e-5;
     int factor_method = WUST_FACTOR_DEFAULT;
+    int sweep_method = WUST_SWEEP_DEFAULT;
     double f = 0, sgn = -1, a0 = 0, L = 0, vmin = 0, vmax = 0;
     int ldr9 = 0;
     double dt = 0, cr = 0;
@@ -139,6 +140,14 @@ struct wust_solver {
     unsigned *tc_sync = nullptr;
     int *tc_err = nullptr;
     TcSweepGeom tc_geom{};
+    // column-chunked tensor-core sweeps (TF32 profile, default): packed
+    // -Lambda_c pages, per-group B chunks, chunk and boundary states, counters
+    bool use_chunks = false;
+    TcChunkGeom ck_geom{};
+    uint8_t *ck_lpack = nullptr, *ck_b = nullptr;
+    float *ck_z = nullptr, *ck_sb = nullptr;
+    unsigned *ck_sync = nullptr;
+    TcChunkBuffers chunk_buffers() const { return TcChunkBuffers{ck_lpack, ck_b, ck_z, ck_sb, ck_sync, tc_err}; }
     // Newton-Schulz factorization (TF32 profile)
     void *ns_scratch = nullptr;
     NsGeom ns_g{};
@@ -188,7 +197,8 @@ static void free_solver(wust_solver *s) {
     void *ptrs[] = {s->vel, s->atten, s->exi, s->eyi, s->mult, s->status, s->invT, s->fscratch, s->u, s->lam,
                     s->tmp, s->work, s->x64, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
                     s->rx_at, s->Yd, s->maskd, s->resid, s->scale, s->loss_src, s->grad, s->dir, s->ret_u,
-                    s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err, s->ns_scratch};
+                    s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err, s->ns_scratch,
+                    s->ck_lpack, s->ck_b, s->ck_z, s->ck_sb, s->ck_sync};
     for (void *p : ptrs) dfree(p);
     for (int i = 0; i < 9; ++i) { dfree(s->c128[i]); dfree(s->c64[i]); }
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
@@ -265,8 +275,10 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
     } else {
         factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
     }
-    if (s->precision == WUST_PRECISION_TF32_REFINED)
+    if (s->precision == WUST_PRECISION_TF32_REFINED) {
         tc_pack_invT(s->invT, s->ny, s->nx, s->tc_geom, s->tc_afwd, s->tc_aadj, st);
+        if (s->use_chunks) tc_chunk_prepare(s->coefs64(), s->tc_afwd, s->tc_aadj, s->ck_geom, s->chunk_buffers(), st);
+    }
     WUST_CUDA(cudaEventRecord(s->ev[2], st));
     int astat = 0;
     WUST_CUDA(cudaMemcpyAsync(&astat, s->status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -310,8 +322,12 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
 static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
     WUST_CUDA(cudaEventRecord(s->sw_ev[0], s->st));
     if (s->precision == WUST_PRECISION_TF32_REFINED) {
-        tc_sweep_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->tc_geom, src, S, adjoint, out, s->tc_b,
-                       s->tc_part, s->tc_sync, s->tc_err, s->st);
+        if (s->use_chunks)
+            tc_chunk_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->ck_geom, s->chunk_buffers(), src, S, adjoint,
+                           out, s->st);
+        else
+            tc_sweep_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->tc_geom, src, S, adjoint, out, s->tc_b,
+                           s->tc_part, s->tc_sync, s->tc_err, s->st);
     } else {
         sweep_solve(s->coefs64(), s->invT, src, S, adjoint, out, s->tmp, s->st);
     }
@@ -527,6 +543,9 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         if (o->factor_method < WUST_FACTOR_DEFAULT || o->factor_method > WUST_FACTOR_GAUSS_JORDAN)
             fail(WUST_ERR_INVALID_INPUT, "unknown factor_method %d", o->factor_method);
         s->factor_method = o->factor_method;
+        if (o->sweep_method < WUST_SWEEP_DEFAULT || o->sweep_method > WUST_SWEEP_SEQUENTIAL)
+            fail(WUST_ERR_INVALID_INPUT, "unknown sweep_method %d", o->sweep_method);
+        s->sweep_method = o->sweep_method;
         s->precision = o->precision;
         s->refine_max = o->refine_max_iters > 0 ? o->refine_max_iters : 8;
         s->refine_tol = o->refine_tol > 0 ? o->refine_tol : 1e-5;
@@ -599,6 +618,19 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
             }
             s->tc_err = dalloc<int>(4);
             WUST_CUDA(cudaMemset(s->tc_err, 0, 4 * sizeof(int)));
+            if (s->sweep_method == WUST_SWEEP_DEFAULT) {
+                s->ck_geom = tc_chunk_geom(ny, nx, tc_chunk_max_ctas());
+                s->use_chunks = s->ck_geom.C >= 2;   // one chunk: the sequential kernel is faster
+            }
+            if (s->use_chunks) {
+                if (s->ck_geom.lpack_bytes) s->ck_lpack = dalloc<uint8_t>(s->ck_geom.lpack_bytes);
+                s->ck_b = dalloc<uint8_t>(s->ck_geom.b_bytes);
+                s->ck_z = dalloc<float>(s->ck_geom.state_bytes / sizeof(float));
+                s->ck_sb = dalloc<float>(s->ck_geom.state_bytes / sizeof(float));
+                WUST_CUDA(cudaMemset(s->ck_z, 0, s->ck_geom.state_bytes));
+                WUST_CUDA(cudaMemset(s->ck_sb, 0, s->ck_geom.state_bytes));
+                s->ck_sync = dalloc<unsigned>(s->ck_geom.sync_words);
+            }
         }
         assemble_and_factor(s, vel, atten);
         *out = s;

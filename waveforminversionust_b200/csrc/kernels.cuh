@@ -50,6 +50,32 @@ void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t 
                     const SrcView &src, int S, bool adjoint, float2 *u, uint8_t *bglob, float *part, unsigned *sync,
                     int *err, cudaStream_t st);
 
+// ---- tcchunk.cu (column-chunked tensor-core sweeps, TF32 inputs) -----------
+struct TcChunkGeom {
+    int n, mt, kc;        // interior size, 64-row M tiles, 16-row K chunks (same packing as TcSweepGeom)
+    int C;                // column chunks per substitution
+    size_t page_bytes;    // packed operand bytes per page
+    size_t lpack_bytes;   // packed -Lambda_c pages: 4 substitutions x C pages
+    size_t b_bytes;       // packed B chunks of C groups
+    size_t state_bytes;   // C column states (re, im planes of 256 sources x ny rows)
+    int sync_words;       // group counters
+};
+struct TcChunkBuffers {
+    uint8_t *lpack, *bglob;
+    float *zst, *sb;      // zero-initialised once (border rows are never written)
+    unsigned *sync;
+    int *err;
+};
+TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas);
+int tc_chunk_max_ctas();
+size_t tc_chunk_state_floats(int ny);
+// Composed propagators of the chunks of all four substitutions (after tc_pack_invT).
+void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
+                      const TcChunkBuffers &b, cudaStream_t st);
+// Same contract as tc_sweep_solve: u (ny*nx*S) is overwritten.
+void tc_chunk_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
+                    const TcChunkBuffers &b, const SrcView &src, int S, bool adjoint, float2 *u, cudaStream_t st);
+
 // ---- nsfactor.cu (Newton-Schulz Schur inverses, TF32 tensor cores) ---------
 struct NsGeom {
     int n, mt, ntn, kc, ks, per;   // ks == 0: the grid does not fit; Gauss-Jordan only

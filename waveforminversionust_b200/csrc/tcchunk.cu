@@ -1,0 +1,803 @@
+// Chunked tensor-core sweeps: the column recurrence of each substitution of
+// applyBlockLU (Runtime/solver/applyBlockLU.cu:433-467) cut into C chunks of
+// columns that run concurrently.
+//
+// Step by step, every substitution is an affine recurrence on one column
+// state c (ny x S):  c_i = Lambda_i c_{i-1} + g_i,  Lambda_i = -+ invT_j W_i
+// (W_i the tridiagonal coupling block of the step, g_i the source or the
+// already-solved column).  Cutting the nx - 1 steps of a substitution into C
+// chunks of consecutive steps:
+//   pass 1    every chunk runs its steps from c = 0, chunk 0 from its true
+//             incoming state (it also writes its columns of u): end states z_c;
+//   boundary  s_0 = z_0,  s_c = z_c + Lambda_c s_{c-1}  for c = 1 .. C-2,
+//             Lambda_c the chunk's composed propagator (formed once per
+//             factorization by running the chunk on the identity);
+//   pass 2    chunks 1 .. C-1 rerun from s_{c-1} and write their columns.
+// The serial depth drops from nx - 1 steps to about 2 (nx - 1) / C + C.
+//
+// A group of mt CTAs (one per 64-row complex M tile, one CTA per SM) runs a
+// chunk.  Each step is one full-K complex GEMM per CTA,
+//     C (64 rows x N) = A (64 rows x n) B (n x N),  N <= 256 sources,
+// real-split with re/im interleaved along K exactly as in tcsweep.cu; A (the
+// packed invT page) and B (the packed right-hand side) stream through a
+// 4-stage bulk-copy ring into kind::tf32 MMAs of N columns, the accumulator
+// sits in tensor memory.  After the MMAs each CTA writes its rows of the new
+// state (re and im planes, rows fastest) and of u, meets its group on a
+// counter barrier, evaluates the next step's stencil for its rows (the
+// neighbour rows come from L2) into the packed B chunks, and meets the group
+// again.  The A chunks of the next step are copied while that happens.
+// Groups never wait on each other.  Every device wait is bounded and reports
+// its site through *err.
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "tc.cuh"
+#include "tcstep.cuh"
+
+namespace wust {
+
+constexpr int kCkThreads = 256;
+constexpr int kCkStages = 4;
+constexpr int kCkMaxN = 256;                                     // sources per launch (MMA N)
+constexpr int kCkRowsPerChunk = 16;                              // complex rows per K chunk
+constexpr int kCkMaxChunks = 148;
+constexpr size_t kCkBSlot = (size_t)kCkMaxN * tc::kChunkBytes;   // 32 KB
+constexpr size_t kCkSmemRing = (size_t)kCkStages * (tc::kAChunk + kCkBSlot);
+constexpr size_t kCkSmemHalo = 2 * kCkMaxN * sizeof(float2);
+constexpr size_t kCkSmemW = 3 * 64 * sizeof(float2);
+constexpr size_t kCkSmem = kCkSmemRing + kCkSmemHalo + kCkSmemW + 256;
+static_assert((size_t)kCkStages * kCkBSlot >= (size_t)kCkMaxN * 64 * sizeof(float2), "B stages hold the staged state");
+static_assert(kCkSmem <= 232448, "shared memory of one CTA");
+
+using tc::chunk_off;
+using tc::to_tf32;
+
+// Launch kinds and the kind of work of one group.
+enum CkPass { CK_FIRST = 0, CK_SECOND = 1, CK_PROP = 2, CK_BOUNDARY = 3 };
+enum CkKind { K_EXACT = 0, K_LOCAL = 1, K_PROP = 2, K_BOUND = 3 };
+// Where the incoming state of a chunk comes from.
+enum CkIn { IN_ZERO = 0, IN_PLANES = 1, IN_UCOL = 2, IN_IDENT = 3 };
+// What produce makes of the staged state.
+enum CkProduce { P_STENCIL = 0, P_IDENT = 1, P_TURN = 2 };
+
+size_t tc_chunk_state_floats(int ny) { return (size_t)2 * kCkMaxN * ny; }
+
+TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas) {
+    TcChunkGeom g{};
+    g.n = ny - 2;
+    g.mt = ceil_div(g.n, 64);
+    g.kc = ceil_div(g.n, kCkRowsPerChunk);
+    const int steps = nx - 1;
+    if (steps < 1 || g.n < 1) fail(WUST_ERR_INVALID_INPUT, "chunked sweep needs Nx >= 2 and Ny >= 3");
+    if (g.mt > max_ctas)
+        fail(WUST_ERR_INVALID_INPUT, "chunked sweep needs %d co-resident CTAs (device holds %d)", g.mt, max_ctas);
+    // about sqrt(2 steps) chunks balance the two passes against the boundary
+    // chain; every chunk keeps at least 2 steps (the mirrored H^H backward
+    // cuts then leave no chunk empty)
+    int C = (int)std::lround(std::sqrt(2.0 * steps));
+    C = std::max(1, std::min({C, max_ctas / g.mt, steps / 2, kCkMaxChunks}));
+    g.C = C;
+    g.page_bytes = (size_t)g.mt * g.kc * tc::kAChunk;
+    g.lpack_bytes = C >= 3 ? (size_t)4 * C * g.page_bytes : 0;
+    g.b_bytes = (size_t)C * g.kc * kCkBSlot;
+    g.state_bytes = (size_t)C * tc_chunk_state_floats(ny) * sizeof(float);
+    g.sync_words = C;
+    return g;
+}
+
+// Optional phase timer (SM cycles of CTA 0, summed over steps, per launch
+// kind), built only into profiling builds of the library.
+#ifdef WUST_CHUNK_PROFILE
+__device__ unsigned long long g_chunk_prof[4][8];
+#define CPROF(k)                                                                                  \
+    do {                                                                                          \
+        if (blockIdx.x == 0 && threadIdx.x == 0) {                                                \
+            const long long t_ = clock64();                                                       \
+            g_chunk_prof[p.pass][k] += (unsigned long long)(t_ - prof_t);                         \
+            prof_t = t_;                                                                          \
+        }                                                                                         \
+    } while (0)
+extern "C" int wust_chunk_profile_read(unsigned long long *out) {
+    return (int)cudaMemcpyFromSymbol(out, g_chunk_prof, sizeof(g_chunk_prof));
+}
+extern "C" int wust_chunk_profile_reset() {
+    unsigned long long z[32] = {};
+    return (int)cudaMemcpyToSymbol(g_chunk_prof, z, sizeof(z));
+}
+#else
+#define CPROF(k) ((void)0)
+#endif
+
+struct ChunkParams {
+    const uint8_t *apack;     // packed pages of the solve (invT or invT^H): [page][mt][kc] chunks
+    const uint8_t *lpack;     // boundary launches: packed -Lambda_c pages, [chunk][mt][kc]
+    size_t page_bytes;
+    Coefs<float2> co;
+    SrcView src;
+    float2 *u;                // [ny, nx, S] (global source index)
+    uint8_t *bglob;           // [group][kc] chunks of N x 128 bytes
+    float *zst;               // [chunk] states: re plane [kCkMaxN][ny], im plane [kCkMaxN][ny]
+    float *sb;                // [chunk] boundary states s_c (c >= 1), same layout
+    unsigned *group_ctr;      // [group]
+    int *err;
+    int ny, nx, n, mt, kc, N;
+    int s0, s_end;            // global sources [s0, s_end) of this launch
+    int half;                 // 0: forward substitution (steps 0 .. nx-2), 1: backward
+    int pass, C;
+    int bounds[kCkMaxChunks + 1];   // first step (within the half) of each chunk
+    unsigned long long timeout_ns;
+};
+
+template <bool ADJ>
+__global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_constant__ ChunkParams p) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *sA = smem;                                          // [stage] 16 KB
+    uint8_t *sB = smem + (size_t)kCkStages * tc::kAChunk;        // [stage] 32 KB
+    // Between a step's MMAs and the next step's B copies the B stages hold the
+    // state of this CTA's 64 rows: cs[s * 64 + row] (complex).
+    float2 *cs = reinterpret_cast<float2 *>(sB);
+    float2 *halo = reinterpret_cast<float2 *>(smem + kCkSmemRing);  // [2][kCkMaxN]: rows 64t-1 and 64t+64
+    float2 *wts = halo + 2 * kCkMaxN;                                // [3][64] stencil weights of own rows
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kCkSmemRing + kCkSmemHalo + kCkSmemW);
+    uint64_t *empty = full + kCkStages;
+    uint64_t *done = empty + kCkStages;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *s_ok = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = blockIdx.x / p.mt, t = blockIdx.x % p.mt;
+    const int ny = p.ny, nx = p.nx, n = p.n, kc = p.kc, N = p.N;
+    const size_t plane = (size_t)ny * nx;
+    const size_t sfl = (size_t)2 * kCkMaxN * ny;                 // floats per state
+    const size_t bbytes = (size_t)N * tc::kChunkBytes;
+    uint8_t *bg = p.bglob + (size_t)g * kc * bbytes;
+    unsigned *ctr = p.group_ctr + g;
+    const int row0 = 64 * t;                                     // first complex interior row of this CTA
+
+    // this group's chunk, kind and steps
+    int chunk, kind, t0, nsteps;
+    if (p.pass == CK_BOUNDARY) {
+        chunk = 0; kind = K_BOUND; t0 = 1; nsteps = p.C - 2;
+    } else {
+        chunk = (p.pass == CK_FIRST ? 0 : 1) + g;
+        kind = p.pass == CK_PROP ? K_PROP : (p.pass == CK_SECOND || chunk == 0) ? K_EXACT : K_LOCAL;
+        t0 = p.bounds[chunk];
+        nsteps = p.bounds[chunk + 1] - t0;
+    }
+    // state planes of the boundary sequence: s_0 = z_0 (the end state of
+    // chunk 0), s_c in sb.  H^H solves carry B states between chunks (the
+    // first B of the next chunk), kept in sb from the start.
+    auto bstate = [&](int c) -> float * { return (c == 0 && !ADJ) ? p.zst : p.sb + (size_t)c * sfl; };
+
+    auto col_of = [&](int k, bool &fwd) -> int {
+        if (kind == K_BOUND) { fwd = false; return 0; }
+        return step_col(p.half * (nx - 1) + t0 + k, nx, fwd);
+    };
+    auto apage = [&](int k) -> const uint8_t * {
+        if (kind == K_BOUND) return p.lpack + (size_t)(t0 + k) * p.page_bytes;
+        bool f;
+        const int j = col_of(k, f);
+        return p.apack + (size_t)((ADJ && f) ? j - 1 : j) * p.page_bytes;
+    };
+    // incoming state value at grid row y (0 .. ny-1; 0 outside), local source s
+    auto cval = [&](int in, const float *pl, int y, int s) -> float2 {
+        if (y < 0 || y >= ny) return f2(0.f, 0.f);
+        if (in == IN_PLANES) return f2(__ldcg(pl + (size_t)s * ny + y), __ldcg(pl + (size_t)(kCkMaxN + s) * ny + y));
+        if (in == IN_UCOL) return __ldcg(p.u + plane * (p.s0 + s) + (size_t)ny * (nx - 1) + y);
+        if (in == IN_IDENT) return f2((y >= 1 && y <= n && y - 1 == p.s0 + s) ? 1.f : 0.f, 0.f);
+        return f2(0.f, 0.f);
+    };
+    // staged state at complex interior row yp (row0 - 1 .. row0 + 64)
+    auto cs_get = [&](int yp, int s) -> float2 {
+        const int l = yp - row0;
+        if (l >= 0 && l < 64) return cs[s * 64 + l];
+        if (l == -1) return halo[s];
+        if (l == 64) return halo[kCkMaxN + s];
+        return f2(0.f, 0.f);
+    };
+    // own rows and halo rows of an incoming state -> shared memory
+    auto stage_in = [&](int in, const float *pl) {
+        __syncthreads();
+        for (int it0 = tid; it0 < 64 * N; it0 += 4 * kCkThreads) {
+            float2 v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int it = it0 + q * kCkThreads;
+                v[q] = it < 64 * N ? cval(in, pl, row0 + (it & 63) + 1, it >> 6) : f2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int it = it0 + q * kCkThreads;
+                if (it < 64 * N) cs[(it >> 6) * 64 + (it & 63)] = v[q];
+            }
+        }
+        for (int it = tid; it < 2 * N; it += kCkThreads) {
+            const int e = it / N, s = it % N;
+            halo[e * kCkMaxN + s] = cval(in, pl, e == 0 ? row0 : row0 + 65, s);
+        }
+    };
+    // halo rows (the neighbours' edge rows) from the state planes
+    auto stage_halo = [&](const float *pl) {
+        __syncthreads();
+        for (int it = tid; it < 2 * N; it += kCkThreads) {
+            const int e = it / N, s = it % N;
+            halo[e * kCkMaxN + s] = cval(IN_PLANES, pl, e == 0 ? row0 : row0 + 65, s);
+        }
+    };
+
+    // B of step k for this CTA's rows from the staged state:
+    //   P_STENCIL  B = base - stencil(state), into the packed chunks, or as
+    //              FP32 planes into `out` (a chunk's outgoing B state);
+    //   P_IDENT    B = state (an incoming B state, or a boundary step);
+    //   P_TURN     the turn of the H^H solve: u(:, nx-1) = SRC_{nx-1} -
+    //              U_{nx-2}^H c on every row, no B.
+    // Exact H^H forward steps also write B into u(:, j-1) (stencil mode:
+    // with its border rows).  Warp w handles sources w, w+8, ...; lane r the
+    // rows 2r, 2r+1 (neighbour rows by shuffles).
+    auto produce = [&](int k, int mode, float *out) {
+        bool fwd1 = true;
+        int j1 = nx;
+        if (mode != P_TURN) j1 = col_of(k, fwd1);
+        const bool pack = mode != P_TURN && !out;
+        const bool ident = mode == P_IDENT;
+        const bool wu = kind == K_EXACT && ADJ && fwd1 && !out;
+        const bool has_base = (kind == K_EXACT || kind == K_LOCAL) && !ident;
+        __syncthreads();
+        if (tid < 64) {
+            const int yp = row0 + tid, y = yp + 1;
+            float2 wc = f2(0.f, 0.f), wm = wc, wp = wc;
+            if (yp < n) {
+                if (ident) wc = f2(-1.f, 0.f);
+                else step_weights<ADJ>(p.co, fwd1, j1, y, wc, wm, wp);
+            }
+            wts[tid] = wc;
+            wts[64 + tid] = wm;
+            wts[128 + tid] = wp;
+        }
+        __syncthreads();
+        const int yp0 = row0 + 2 * lane, y0 = yp0 + 1;
+        const bool v0 = yp0 < n, v1 = yp0 + 1 < n;
+        const bool in_k = yp0 < kCkRowsPerChunk * kc;
+        const float2 wc0 = wts[2 * lane], wm0 = wts[64 + 2 * lane], wp0 = wts[128 + 2 * lane];
+        const float2 wc1 = wts[2 * lane + 1], wm1 = wts[64 + 2 * lane + 1], wp1 = wts[128 + 2 * lane + 1];
+        for (int sb0 = warp; sb0 < N; sb0 += 4 * 8) {
+            float2 base[4][2];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int s = sb0 + 8 * q, gs = p.s0 + s;
+                base[q][0] = base[q][1] = f2(0.f, 0.f);
+                if (has_base && s < N && gs < p.s_end) {
+                    if (v0) base[q][0] = step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y0, gs);
+                    if (v1) base[q][1] = step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y0 + 1, gs);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int s = sb0 + 8 * q, gs = p.s0 + s;
+                if (s >= N) break;                                   // warp-uniform
+                const float4 cv = *reinterpret_cast<const float4 *>(cs + s * 64 + 2 * lane);
+                const float2 c0 = f2(cv.x, cv.y), c1 = f2(cv.z, cv.w);
+                float2 cm = f2(__shfl_up_sync(0xffffffffu, c1.x, 1), __shfl_up_sync(0xffffffffu, c1.y, 1));
+                float2 cp = f2(__shfl_down_sync(0xffffffffu, c0.x, 1), __shfl_down_sync(0xffffffffu, c0.y, 1));
+                if (lane == 0) cm = halo[s];
+                if (lane == 31) cp = halo[kCkMaxN + s];
+                float2 b0 = f2(0.f, 0.f), b1 = b0;
+                if (gs < p.s_end) {
+                    if (v0) {
+                        float2 acc = cmul(wc0, c0);
+                        cfma(acc, wm0, cm);
+                        cfma(acc, wp0, c1);
+                        b0 = csub(base[q][0], acc);
+                        if (wu) p.u[plane * gs + (size_t)ny * (j1 - 1) + y0] = b0;
+                    }
+                    if (v1) {
+                        float2 acc = cmul(wc1, c1);
+                        cfma(acc, wm1, c0);
+                        cfma(acc, wp1, cp);
+                        b1 = csub(base[q][1], acc);
+                        if (wu) p.u[plane * gs + (size_t)ny * (j1 - 1) + y0 + 1] = b1;
+                    }
+                }
+                if (out) {
+                    float *re = out + (size_t)s * ny, *im = out + (size_t)(kCkMaxN + s) * ny;
+                    if (v0 && gs < p.s_end) { __stcg(re + y0, b0.x); __stcg(im + y0, b0.y); }
+                    if (v1 && gs < p.s_end) { __stcg(re + y0 + 1, b1.x); __stcg(im + y0 + 1, b1.y); }
+                } else if (pack && in_k) {
+                    const int Q = yp0 / kCkRowsPerChunk, yl = yp0 % kCkRowsPerChunk;
+                    *reinterpret_cast<float4 *>(bg + (size_t)Q * bbytes + chunk_off(s, 2 * yl)) =
+                        make_float4(to_tf32(b0.x), to_tf32(b0.y), to_tf32(b1.x), to_tf32(b1.y));
+                }
+            }
+        }
+        if (wu && !ident) {
+            // border rows 0 and ny-1 of u(:, j1-1) (no B entry)
+            for (int it = tid; it < 2 * N; it += kCkThreads) {
+                const int e = it / N, s = it % N, gs = p.s0 + s;
+                if ((e == 0 && t != 0) || (e == 1 && t != p.mt - 1) || gs >= p.s_end) continue;
+                const int y = e == 0 ? 0 : ny - 1, yp = y - 1;
+                float2 wc, wm, wp;
+                step_weights<ADJ>(p.co, fwd1, j1, y, wc, wm, wp);
+                float2 acc = cmul(wc, cs_get(yp, s));
+                cfma(acc, wm, cs_get(yp - 1, s));
+                cfma(acc, wp, cs_get(yp + 1, s));
+                p.u[plane * gs + (size_t)ny * (j1 - 1) + y] =
+                    csub(step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y, gs), acc);
+            }
+        }
+    };
+
+    if (tid == 0) {
+        for (int q = 0; q < kCkStages; ++q) {
+            tc::mbar_init(&full[q], 2);       // A copy + B copy
+            tc::mbar_init(&empty[q], 1);      // MMAs of the stage retired
+        }
+        tc::mbar_init(done, 1);
+        tc::mbar_fence_init();
+    }
+    const uint32_t tcols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+    if (warp == 0) tc::tmem_alloc(tmem_slot, tcols);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    // Accumulator (TMEM) -> staged state, own rows (rows beyond the grid 0).
+    auto drain_tmem = [&]() {
+        const int l = 32 * (warp & 3) + lane;
+        const int part = l >> 6;                       // TMEM lanes 0-63: real parts, 64-127: imaginary
+        const int row = l & 63;
+        const bool row_ok = row0 + row < n;
+        const int hc = N / 2, c0 = (warp >> 2) * hc;
+        float *csf = reinterpret_cast<float *>(cs);
+        const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+        int cb = 0;
+        for (; cb + 32 <= hc; cb += 32) {
+            float v[32];
+            tc::tmem_ld32(tl + (uint32_t)(c0 + cb), v);
+#pragma unroll
+            for (int q = 0; q < 32; ++q) csf[((size_t)(c0 + cb + q) * 64 + row) * 2 + part] = row_ok ? v[q] : 0.f;
+        }
+        for (; cb < hc; cb += 8) {
+            float v[8];
+            tc::tmem_ld8(tl + (uint32_t)(c0 + cb), v);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) csf[((size_t)(c0 + cb + q) * 64 + row) * 2 + part] = row_ok ? v[q] : 0.f;
+        }
+    };
+    // The state after step k: subtracting steps take old - value; write the
+    // finished columns of u, and the state's edge rows (every row on the
+    // chunk's last step) to the planes curp.
+    auto finish = [&](int k, float *curp, bool last) {
+        bool fwd = false;
+        const int j = col_of(k, fwd);
+        const bool sub = kind == K_BOUND || (!ADJ && !fwd);
+        const bool wu = kind == K_EXACT && (!ADJ || !fwd);
+        const float *oldp = kind == K_BOUND ? (ADJ ? p.sb : p.zst) + (size_t)(t0 + k) * sfl : nullptr;
+        const bool old_u = sub && kind != K_BOUND && kind != K_PROP;
+        const int yp0 = row0 + 2 * lane, y0 = yp0 + 1;
+        const bool v0 = yp0 < n, v1 = yp0 + 1 < n;
+        __syncthreads();
+        for (int sb0 = warp; sb0 < N; sb0 += 4 * 8) {
+            float2 o[4][2];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int s = sb0 + 8 * q, gs = p.s0 + s;
+                o[q][0] = o[q][1] = f2(0.f, 0.f);
+                if (s < N && gs < p.s_end) {
+                    if (old_u) {
+                        const float2 *uc = p.u + plane * gs + (size_t)ny * j;
+                        if (v0) o[q][0] = __ldcg(uc + y0);
+                        if (v1) o[q][1] = __ldcg(uc + y0 + 1);
+                    } else if (kind == K_BOUND) {
+                        if (v0) o[q][0] = f2(__ldcg(oldp + (size_t)s * ny + y0), __ldcg(oldp + (size_t)(kCkMaxN + s) * ny + y0));
+                        if (v1)
+                            o[q][1] = f2(__ldcg(oldp + (size_t)s * ny + y0 + 1),
+                                         __ldcg(oldp + (size_t)(kCkMaxN + s) * ny + y0 + 1));
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int s = sb0 + 8 * q, gs = p.s0 + s;
+                if (s >= N) break;                                   // warp-uniform
+                float4 *cp4 = reinterpret_cast<float4 *>(cs + s * 64 + 2 * lane);
+                float4 cv = *cp4;
+                if (sub) {
+                    cv = make_float4(o[q][0].x - cv.x, o[q][0].y - cv.y, o[q][1].x - cv.z, o[q][1].y - cv.w);
+                    if (!v0) { cv.x = 0.f; cv.y = 0.f; }
+                    if (!v1) { cv.z = 0.f; cv.w = 0.f; }
+                    *cp4 = cv;
+                }
+                if (gs >= p.s_end) continue;
+                if (wu) {
+                    float2 *uc = p.u + plane * gs + (size_t)ny * j;
+                    if (v0) uc[y0] = f2(cv.x, cv.y);
+                    if (v1) uc[y0 + 1] = f2(cv.z, cv.w);
+                }
+                float *re = curp + (size_t)s * ny, *im = curp + (size_t)(kCkMaxN + s) * ny;
+                if (v0 && (last || lane == 0)) { __stcg(re + y0, cv.x); __stcg(im + y0, cv.y); }
+                if (v1 && (last || lane == 31)) { __stcg(re + y0 + 1, cv.z); __stcg(im + y0 + 1, cv.w); }
+            }
+        }
+        if (kind == K_EXACT && ADJ && !fwd && t == 0) {
+            // H^H backward: border rows of u(:, j) are zero
+            for (int s = tid; s < N; s += kCkThreads) {
+                const int gs = p.s0 + s;
+                if (gs >= p.s_end) continue;
+                p.u[plane * gs + (size_t)ny * j] = f2(0.f, 0.f);
+                p.u[plane * gs + (size_t)ny * j + ny - 1] = f2(0.f, 0.f);
+            }
+        }
+    };
+
+    // Warps 1-7, while the MMAs run: pull into L2 the field columns that the
+    // coming finish (old column of a subtracting step) and produce (base of
+    // the next step) will read, own rows of every source.
+    auto prefetch_cols = [&](int k) {
+        const float2 *cols[2] = {nullptr, nullptr};
+        bool fwd;
+        const int j = col_of(k, fwd);
+        if ((kind == K_EXACT || kind == K_LOCAL) && !ADJ && !fwd) cols[0] = p.u + (size_t)ny * j;
+        if ((kind == K_EXACT || kind == K_LOCAL) && k + 1 < nsteps) {
+            bool f1;
+            const int j1 = col_of(k + 1, f1);
+            if (ADJ && !f1) cols[1] = p.u + (size_t)ny * j1;
+            else if (p.src.mode == SRC_DENSE && (!ADJ || j1 >= 2) && f1)
+                cols[1] = p.src.dense + (size_t)ny * (ADJ ? j1 - 1 : j1);
+        }
+        const int y_first = row0 + 1, y_last = min(row0 + 64, n);
+        for (int c = 0; c < 2; ++c) {
+            if (!cols[c]) continue;
+            for (int it = tid - 32; it < N * 5; it += kCkThreads - 32) {
+                const int s = it / 5, q = it % 5, gs = p.s0 + s;
+                if (gs >= p.s_end) continue;
+                const char *first = reinterpret_cast<const char *>(cols[c] + plane * gs + y_first);
+                const char *last = reinterpret_cast<const char *>(cols[c] + plane * gs + y_last);
+                const uintptr_t line = ((uintptr_t)first >> 7) + (uintptr_t)q;
+                if (line > ((uintptr_t)last >> 7)) continue;
+                const char *a = q == 0 ? first : reinterpret_cast<const char *>(line << 7);
+                tc::prefetch_l2(a);
+            }
+        }
+    };
+
+    // ---- bulk-copy ring (thread 0); chunk ci = k * kc + q of step k --------
+    uint32_t a_next = 0, b_next = 0, retired = 0, full_waited = 0;
+    auto pump = [&](int k, bool b_ready) {
+        const uint32_t a_end = (uint32_t)min(k + 2, nsteps) * (uint32_t)kc;
+        while (a_next < a_end && a_next < retired + kCkStages) {
+            const int ks = (int)(a_next / kc), q = (int)(a_next % kc), slot = (int)(a_next % kCkStages);
+            tc::mbar_expect_tx(&full[slot], tc::kAChunk);
+            tc::bulk_g2s(sA + (size_t)slot * tc::kAChunk, apage(ks) + ((size_t)t * kc + q) * tc::kAChunk, tc::kAChunk,
+                         &full[slot]);
+            ++a_next;
+        }
+        if (b_ready) {
+            const uint32_t b_end = (uint32_t)(k + 1) * (uint32_t)kc;
+            while (b_next < b_end && b_next < a_next) {
+                const int q = (int)(b_next % kc), slot = (int)(b_next % kCkStages);
+                tc::mbar_expect_tx(&full[slot], (uint32_t)bbytes);
+                tc::bulk_g2s(sB + (size_t)slot * kCkBSlot, bg + (size_t)q * bbytes, (uint32_t)bbytes, &full[slot]);
+                ++b_next;
+            }
+        }
+    };
+
+    unsigned epoch = 0;
+    bool ok = nsteps > 0;
+    if (ok) {
+        if (tid == 0) pump(0, false);
+        int in0 = IN_ZERO, mode0 = P_STENCIL;
+        const float *pl0 = nullptr;
+        if (kind == K_EXACT && chunk > 0) {
+            in0 = IN_PLANES;
+            pl0 = bstate(chunk - 1);
+            if (ADJ) mode0 = P_IDENT;                      // the incoming state is this chunk's first B
+        } else if (kind == K_EXACT && p.half == 1) {
+            in0 = IN_UCOL;
+        } else if (kind == K_PROP) {
+            in0 = IN_IDENT;
+        } else if (kind == K_BOUND) {
+            in0 = IN_PLANES;
+            pl0 = bstate(0);
+            mode0 = P_IDENT;
+        } else if (kind == K_LOCAL && ADJ) {
+            mode0 = P_IDENT;                               // first B = 0
+        }
+        stage_in(in0, pl0);
+        produce(0, mode0, nullptr);
+        epoch += (unsigned)p.mt;
+        ok = counter_sync(ctr, epoch, p.err, s_ok, p.timeout_ns, SITE_B);
+    }
+    float *cur = kind == K_BOUND ? nullptr : p.zst + (size_t)chunk * sfl;
+    constexpr int kMmaPerChunk = tc::kChunkBytes / 32;
+    const uint32_t idesc = tc::instr_desc<true>(tc::kTileRows, N);
+
+#ifdef WUST_CHUNK_PROFILE
+    long long prof_t = clock64();
+    if (blockIdx.x == 0 && tid == 0) g_chunk_prof[p.pass][7] += (unsigned long long)nsteps;
+#endif
+    for (int k = 0; k < nsteps && ok; ++k) {
+        CPROF(6);
+        if (tid == 0) {
+            pump(k, true);
+            bool good = true;
+            for (int q = 0; q < kc; ++q) {
+                const uint32_t ci = (uint32_t)k * kc + q;
+                const int slot = (int)(ci % kCkStages);
+                if (!tc::mbar_wait(&full[slot], (ci / kCkStages) & 1u, p.timeout_ns)) { good = false; break; }
+                full_waited = ci + 1;
+                tc::fence_after();
+#pragma unroll
+                for (int kk = 0; kk < kMmaPerChunk; ++kk)
+                    tc::mma<true>(tmem, tc::smem_desc(sA + (size_t)slot * tc::kAChunk + kk * 256),
+                                  tc::smem_desc(sB + (size_t)slot * kCkBSlot + kk * 256), idesc,
+                                  (q > 0 || kk > 0) ? 1u : 0u);
+                tc::commit(&empty[slot]);
+                if (q >= 1) {
+                    const uint32_t pc = ci - 1;
+                    if (!tc::mbar_wait(&empty[pc % kCkStages], (pc / kCkStages) & 1u, p.timeout_ns)) {
+                        good = false;
+                        break;
+                    }
+                    retired = ci;
+                    pump(k, true);
+                }
+            }
+            tc::commit(done);
+            if (good) {
+                const uint32_t pc = (uint32_t)(k + 1) * kc - 1;
+                if (tc::mbar_wait(&empty[pc % kCkStages], (pc / kCkStages) & 1u, p.timeout_ns)) {
+                    retired = pc + 1;
+                    pump(k, true);          // A chunks of the next step
+                } else {
+                    good = false;
+                }
+            }
+            if (!good) atomicCAS(p.err, 0, SITE_COPY);
+        }
+        if (warp >= 1) prefetch_cols(k);
+        CPROF(0);
+        if (!tc::mbar_wait(done, (uint32_t)(k & 1), p.timeout_ns)) atomicCAS(p.err, 0, SITE_MMA);
+        tc::fence_after();
+        if (tid == 0) *s_ok = (*(volatile int *)p.err == 0);
+        __syncthreads();
+        if (!*s_ok) {
+            ok = false;
+            break;
+        }
+        float *curp = kind == K_BOUND ? bstate(t0 + k) : cur;
+        CPROF(1);
+        drain_tmem();
+        tc::fence_before();
+        finish(k, curp, kind == K_BOUND || k + 1 == nsteps);
+        CPROF(2);
+        epoch += (unsigned)p.mt;
+        if (!counter_sync(ctr, epoch, p.err, s_ok, p.timeout_ns, SITE_GROUP)) {
+            ok = false;
+            break;
+        }
+        tc::fence_after();
+        CPROF(3);
+        if (k + 1 < nsteps) {
+            stage_halo(curp);
+            produce(k + 1, kind == K_BOUND ? P_IDENT : P_STENCIL, nullptr);
+            CPROF(4);
+            epoch += (unsigned)p.mt;
+            if (!counter_sync(ctr, epoch, p.err, s_ok, p.timeout_ns, SITE_B)) {
+                ok = false;
+                break;
+            }
+        } else if (kind == K_EXACT && ADJ && p.half == 0 && t0 + k == nx - 2) {
+            stage_halo(curp);
+            produce(k, P_TURN, nullptr);
+        } else if (ADJ && p.pass == CK_FIRST && chunk + 1 < p.C) {
+            // outgoing B state of the chunk: the first B of the next chunk
+            stage_halo(curp);
+            produce(k + 1, P_STENCIL, bstate(chunk));
+        }
+    }
+
+    // copies issued but never waited for (a failure): stand in for the B
+    // copies that will not come, then let them land (bounded)
+    if (tid == 0) {
+        for (uint32_t ci = full_waited; ci < a_next; ++ci) {
+            const int slot = (int)(ci % kCkStages);
+            if (ci >= b_next) tc::mbar_arrive(&full[slot]);
+            tc::mbar_wait(&full[slot], (ci / kCkStages) & 1u, p.timeout_ns);
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (warp == 0) tc::tmem_dealloc(tmem, tcols);
+}
+
+// -Lambda_c (columns [s0, s_end) of the propagators of chunks 1 .. C-2, in
+// the state planes) -> packed [Ar -Ai; Ai Ar] A pages of the boundary steps
+// (page c), and the rows [s0, s_end) of -Lambda_c^H -> the pages C-1-c of the
+// H^H boundary steps.
+__global__ void pack_lambda_kernel(const float *zst, size_t sfl, int ny, int n, int mt, int kc, size_t page_bytes,
+                                   int s0, int s_end, int C, uint8_t *lpack, uint8_t *lpack_h) {
+    const int i_s = threadIdx.x;                     // stacked row 0..127
+    const int Q = blockIdx.x;                        // K chunk
+    const int m = blockIdx.y;                        // M tile
+    const int c = 1 + blockIdx.z;                    // chunk
+    const int i = m * 64 + (i_s & 63);
+    const bool imrow = i_s >= 64;
+    const float *pl = zst + (size_t)c * sfl;
+    // direct: A(i, k) = -Lambda(i, k) for K columns k in [s0, s_end)
+    if ((Q * kCkRowsPerChunk < s_end || s_end >= n) && (Q + 1) * kCkRowsPerChunk > s0) {
+        uint8_t *dst = lpack + (size_t)c * page_bytes + ((size_t)m * kc + Q) * tc::kAChunk;
+#pragma unroll 2
+        for (int k4 = 0; k4 < 8; ++k4) {
+            float v[4];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = Q * kCkRowsPerChunk + 2 * k4 + h;
+                float2 a = make_float2(0.f, 0.f);
+                if (i < n && k >= s0 && k < s_end) {
+                    const int s = k - s0;
+                    a = make_float2(-pl[(size_t)s * ny + i + 1], -pl[(size_t)(kCkMaxN + s) * ny + i + 1]);
+                }
+                v[2 * h] = imrow ? a.y : a.x;
+                v[2 * h + 1] = imrow ? a.x : -a.y;
+            }
+            const int kk = Q * kCkRowsPerChunk + 2 * k4;   // K columns kk, kk+1 (the last tile also zeroes the padding)
+            if (kk + 1 >= s0 && (kk < s_end || s_end >= n))
+                *reinterpret_cast<float4 *>(dst + chunk_off(i_s, 4 * k4)) =
+                    make_float4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2]), to_tf32(v[3]));
+        }
+    }
+    // conjugate transpose: A(i, k) = -conj(Lambda(k, i)) for rows i in [s0, s_end)
+    if (m * 64 >= s0 && m * 64 < s_end) {
+        uint8_t *dst = lpack_h + (size_t)(C - 1 - c) * page_bytes + ((size_t)m * kc + Q) * tc::kAChunk;
+#pragma unroll 2
+        for (int k4 = 0; k4 < 8; ++k4) {
+            float v[4];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = Q * kCkRowsPerChunk + 2 * k4 + h;
+                float2 a = make_float2(0.f, 0.f);
+                if (i < n && i < s_end && k < n) {
+                    const int s = i - s0;
+                    a = make_float2(-pl[(size_t)s * ny + k + 1], pl[(size_t)(kCkMaxN + s) * ny + k + 1]);
+                }
+                v[2 * h] = imrow ? a.y : a.x;
+                v[2 * h + 1] = imrow ? a.x : -a.y;
+            }
+            *reinterpret_cast<float4 *>(dst + chunk_off(i_s, 4 * k4)) =
+                make_float4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2]), to_tf32(v[3]));
+        }
+    }
+}
+
+static void ck_configure() {
+    static thread_local int configured_device = -1;
+    int dev = 0;
+    WUST_CUDA(cudaGetDevice(&dev));
+    if (configured_device == dev) return;
+    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
+    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
+    configured_device = dev;
+}
+
+int tc_chunk_max_ctas() {
+    ck_configure();
+    int dev = 0, sms = 0, per_sm = 0;
+    WUST_CUDA(cudaGetDevice(&dev));
+    WUST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    WUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc_chunk_kernel<false>, kCkThreads, kCkSmem));
+    return sms * per_sm;
+}
+
+static ChunkParams base_params(const Coefs<float2> &co, const TcChunkGeom &g, const TcChunkBuffers &b) {
+    ChunkParams p{};
+    p.page_bytes = g.page_bytes;
+    p.co = co;
+    p.bglob = b.bglob;
+    p.zst = b.zst;
+    p.sb = b.sb;
+    p.group_ctr = b.sync;
+    p.err = b.err;
+    p.ny = co.ny;
+    p.nx = co.nx;
+    p.n = g.n;
+    p.mt = g.mt;
+    p.kc = g.kc;
+    p.C = g.C;
+    p.timeout_ns = 1000000000ull;
+    return p;
+}
+
+// Chunk bounds (first step within the half) of one substitution.  The
+// forward substitutions cut the columns at F[c] = c (nx-1) / C; the backward
+// ones mirror the cuts so that the composed propagators of the H^H
+// substitutions (which carry B states) are the conjugate transposes of those
+// of the H substitutions: H backward chunk C-1-c covers the pages of the H^H
+// forward chunk c, H^H backward chunk C-1-c the columns of H forward chunk c.
+static void set_bounds(ChunkParams &p, int C, bool adjoint, int half) {
+    const int steps = p.nx - 1;
+    auto F = [&](int c) { return (int)((long long)c * steps / C); };
+    for (int c = 0; c <= C; ++c) {
+        if (half == 0) p.bounds[c] = F(c);
+        else if (!adjoint) p.bounds[c] = steps - F(C - c);
+        else p.bounds[c] = (c == 0 || c == C) ? (c == 0 ? 0 : steps) : steps - 1 - F(C - c);
+    }
+}
+
+static void ck_launch(ChunkParams &p, bool adjoint, int pass, int groups, cudaStream_t st) {
+    if (groups <= 0) return;
+    p.pass = pass;
+    WUST_CUDA(cudaMemsetAsync(p.group_ctr, 0, sizeof(unsigned) * groups, st));
+    void *args[] = {&p};
+    const dim3 grid(groups * p.mt), block(kCkThreads);
+    if (adjoint)
+        WUST_CUDA(cudaLaunchCooperativeKernel((void *)tc_chunk_kernel<true>, grid, block, args, kCkSmem, st));
+    else
+        WUST_CUDA(cudaLaunchCooperativeKernel((void *)tc_chunk_kernel<false>, grid, block, args, kCkSmem, st));
+    ++g_kernel_launches;
+}
+
+static uint8_t *lpack_of(const TcChunkGeom &g, uint8_t *lpack, bool adjoint, int half) {
+    return lpack + (size_t)((adjoint ? 2 : 0) + half) * g.C * g.page_bytes;
+}
+
+void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
+                      const TcChunkBuffers &b, cudaStream_t st) {
+    (void)aadj;
+    ck_configure();
+    if (g.C < 3) return;
+    // source tiles of whole 64-row M tiles (the transposed pack fills M tiles)
+    const int ntile = ceil_div(g.n, kCkMaxN);
+    const int N = std::min(kCkMaxN, ceil_div(ceil_div(g.n, ntile), 64) * 64);
+    ChunkParams p = base_params(co, g, b);
+    const size_t sfl = tc_chunk_state_floats(co.ny);
+    p.apack = afwd;
+    for (int half = 0; half < 2; ++half) {
+        p.half = half;
+        set_bounds(p, g.C, false, half);
+        uint8_t *lp = lpack_of(g, b.lpack, false, half);
+        uint8_t *lph = lpack_of(g, b.lpack, true, 1 - half);
+        for (int s0 = 0; s0 < g.n; s0 += N) {
+            p.s0 = s0;
+            p.s_end = std::min(g.n, s0 + N);
+            p.N = N;
+            ck_launch(p, false, CK_PROP, g.C - 2, st);
+            const dim3 grid(g.kc, g.mt, g.C - 2);
+            pack_lambda_kernel<<<grid, 128, 0, st>>>(b.zst, sfl, co.ny, g.n, g.mt, g.kc, g.page_bytes, s0, p.s_end, g.C,
+                                                     lp, lph);
+            ++g_kernel_launches;
+        }
+    }
+    WUST_LAUNCH_CHECK();
+}
+
+void tc_chunk_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
+                    const TcChunkBuffers &b, const SrcView &src, int S, bool adjoint, float2 *u, cudaStream_t st) {
+    ck_configure();
+    const int ny = co.ny, nx = co.nx;
+    WUST_CUDA(cudaMemsetAsync(u, 0, sizeof(float2) * (size_t)ny * nx * S, st));
+    ChunkParams p = base_params(co, g, b);
+    p.apack = adjoint ? aadj : afwd;
+    p.src = src;
+    p.u = u;
+    for (int s0 = 0; s0 < S; s0 += kCkMaxN) {
+        p.s0 = s0;
+        p.s_end = std::min(S, s0 + kCkMaxN);
+        p.N = ceil_div(p.s_end - s0, 16) * 16;
+        for (int half = 0; half < 2; ++half) {
+            p.half = half;
+            set_bounds(p, g.C, adjoint, half);
+            p.lpack = lpack_of(g, b.lpack, adjoint, half);
+            ck_launch(p, adjoint, CK_FIRST, g.C, st);
+            if (g.C >= 3) ck_launch(p, adjoint, CK_BOUNDARY, 1, st);
+            if (g.C >= 2) ck_launch(p, adjoint, CK_SECOND, g.C - 1, st);
+        }
+    }
+    WUST_LAUNCH_CHECK();
+}
+
+}  // namespace wust

@@ -61,7 +61,7 @@ class HelmholtzSolver:
     def __init__(self, x, y, vel, atten, f, signConvention, a0, L_PML, options, *,
                  precision: str = "c64", refine_tol: float = 1e-5, refine_max_iters: int = 8,
                  max_sources: int | None = None, stream: torch.cuda.Stream | None = None,
-                 factor_method: str = "default"):
+                 factor_method: str = "default", sweep_method: str = "default"):
         if not isinstance(options, dict) or "backend" not in options or "stencil_bounds" not in options:
             raise WustError(1, "Explicit backend and fixed stencil_bounds are required")
         bounds = options["stencil_bounds"]
@@ -103,6 +103,10 @@ class HelmholtzSolver:
         if factor_method not in methods:
             raise WustError(1, f"factor_method must be one of {sorted(methods)}")
         opts.factor_method = methods[factor_method]
+        sweeps = {"default": 0, "sequential": 1}
+        if sweep_method not in sweeps:
+            raise WustError(1, f"sweep_method must be one of {sorted(sweeps)}")
+        opts.sweep_method = sweeps[sweep_method]
         opts.max_sources = int(max_sources or 256)
         self._opts = opts
         self.precision = precision
