@@ -385,19 +385,20 @@ def main():
     if sweep_ms_step >= head["factor_ms"]:
         flop = fl["apply"]
         achieved = flop / (head["sweep_ms_per_launch"] * 1e-3) / 1e12
-        kname = ("tc_sweep_kernel (persistent tcgen05 TF32 block-LU sweep pair, 256 sources)"
+        kname = ("tc_chunk_kernel (column-chunked tcgen05 TF32 block-LU sweep pair, 256 sources: per "
+                 "substitution pass 1 + boundary chain + pass 2 = 3 launches)"
                  if args.precision == "tf32-refined" else "sweep kernels (CUDA-core block-LU sweep pair)")
     else:
         flop = fl["factor"]
         achieved = flop / (head["factor_ms"] * 1e-3) / 1e12
         kname = ("ns_factor_kernel + factor_kernel (Newton-Schulz Schur inverses, Gauss-Jordan pages)"
                  if args.precision == "tf32-refined" else "factor_kernel (Schur recursion + Gauss-Jordan inverses)")
-    # DRAM bytes of one launch of the dominant kernel, measured with ncu
-    # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on this kernel
-    # at 552^2 with 256 sources: 6.91 GB read + 1.22 GB written per sweep pair
+    # DRAM bytes of one sweep pair of the dominant kernel (its six launches),
+    # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one
+    # pass) at 552^2 with 256 sources: 13.61 GB read + 2.74 GB written
     traffic = None
     if flop == fl["apply"] and args.precision == "tf32-refined" and WORKLOAD == "config2":
-        traffic = 8.13e9
+        traffic = 16.34e9
     roofline = dict(kernel=kname, bound="tensor", achieved=achieved, peak=peak_tf, unit="TFLOP/s",
                     frac=achieved / peak_tf, peak_source=peak_src, traffic=traffic,
                     traffic_unit="bytes per launch (ncu)", hbm_gbs_achieved=(

@@ -146,8 +146,9 @@ struct wust_solver {
     TcChunkGeom ck_geom{};
     uint8_t *ck_lpack = nullptr, *ck_b = nullptr;
     float *ck_z = nullptr, *ck_sb = nullptr;
+    float2 *ck_edges = nullptr;
     unsigned *ck_sync = nullptr;
-    TcChunkBuffers chunk_buffers() const { return TcChunkBuffers{ck_lpack, ck_b, ck_z, ck_sb, ck_sync, tc_err}; }
+    TcChunkBuffers chunk_buffers() const { return TcChunkBuffers{ck_lpack, ck_b, ck_z, ck_sb, ck_edges, ck_sync, tc_err}; }
     // Newton-Schulz factorization (TF32 profile)
     void *ns_scratch = nullptr;
     NsGeom ns_g{};
@@ -198,7 +199,7 @@ static void free_solver(wust_solver *s) {
                     s->tmp, s->work, s->x64, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
                     s->rx_at, s->Yd, s->maskd, s->resid, s->scale, s->loss_src, s->grad, s->dir, s->ret_u,
                     s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err, s->ns_scratch,
-                    s->ck_lpack, s->ck_b, s->ck_z, s->ck_sb, s->ck_sync};
+                    s->ck_lpack, s->ck_b, s->ck_z, s->ck_sb, s->ck_edges, s->ck_sync};
     for (void *p : ptrs) dfree(p);
     for (int i = 0; i < 9; ++i) { dfree(s->c128[i]); dfree(s->c64[i]); }
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
@@ -630,6 +631,7 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
                 WUST_CUDA(cudaMemset(s->ck_z, 0, s->ck_geom.state_bytes));
                 WUST_CUDA(cudaMemset(s->ck_sb, 0, s->ck_geom.state_bytes));
                 s->ck_sync = dalloc<unsigned>(s->ck_geom.sync_words);
+                s->ck_edges = dalloc<float2>(s->ck_geom.edge_bytes / sizeof(float2));
             }
         }
         assemble_and_factor(s, vel, atten);

@@ -58,11 +58,13 @@ struct TcChunkGeom {
     size_t lpack_bytes;   // packed -Lambda_c pages: 4 substitutions x C pages
     size_t b_bytes;       // packed B chunks of C groups
     size_t state_bytes;   // C column states (re, im planes of 256 sources x ny rows)
+    size_t edge_bytes;    // first and last state row of every CTA of C groups
     int sync_words;       // group counters
 };
 struct TcChunkBuffers {
     uint8_t *lpack, *bglob;
     float *zst, *sb;      // zero-initialised once (border rows are never written)
+    float2 *edges;
     unsigned *sync;
     int *err;
 };

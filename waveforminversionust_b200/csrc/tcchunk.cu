@@ -38,7 +38,8 @@
 
 namespace wust {
 
-constexpr int kCkThreads = 256;
+constexpr int kCkThreads = 512;
+constexpr int kCkWarps = kCkThreads / 32;
 constexpr int kCkStages = 4;
 constexpr int kCkMaxN = 256;                                     // sources per launch (MMA N)
 constexpr int kCkRowsPerChunk = 16;                              // complex rows per K chunk
@@ -50,6 +51,8 @@ constexpr size_t kCkSmemW = 3 * 64 * sizeof(float2);
 constexpr size_t kCkSmem = kCkSmemRing + kCkSmemHalo + kCkSmemW + 256;
 static_assert((size_t)kCkStages * kCkBSlot >= (size_t)kCkMaxN * 64 * sizeof(float2), "B stages hold the staged state");
 static_assert(kCkSmem <= 232448, "shared memory of one CTA");
+
+__host__ __device__ constexpr int ceil_div8(int x) { return (x + 7) / 8 * 8; }
 
 using tc::chunk_off;
 using tc::to_tf32;
@@ -83,6 +86,7 @@ TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas) {
     g.lpack_bytes = C >= 3 ? (size_t)4 * C * g.page_bytes : 0;
     g.b_bytes = (size_t)C * g.kc * kCkBSlot;
     g.state_bytes = (size_t)C * tc_chunk_state_floats(ny) * sizeof(float);
+    g.edge_bytes = (size_t)C * g.mt * 2 * kCkMaxN * sizeof(float2);
     g.sync_words = C;
     return g;
 }
@@ -120,6 +124,7 @@ struct ChunkParams {
     uint8_t *bglob;           // [group][kc] chunks of N x 128 bytes
     float *zst;               // [chunk] states: re plane [kCkMaxN][ny], im plane [kCkMaxN][ny]
     float *sb;                // [chunk] boundary states s_c (c >= 1), same layout
+    float2 *edges;            // [group][mt][2][kCkMaxN]: first and last own row of each CTA's state
     unsigned *group_ctr;      // [group]
     int *err;
     int ny, nx, n, mt, kc, N;
@@ -218,13 +223,31 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
             halo[e * kCkMaxN + s] = cval(in, pl, e == 0 ? row0 : row0 + 65, s);
         }
     };
-    // halo rows (the neighbours' edge rows) from the state planes
-    auto stage_halo = [&](const float *pl) {
+    // halo rows: the last row of the CTA above and the first row of the CTA
+    // below (zero at the grid's edges)
+    float2 *my_edges = p.edges + ((size_t)g * p.mt + t) * 2 * kCkMaxN;
+    auto stage_halo = [&]() {
         __syncthreads();
         for (int it = tid; it < 2 * N; it += kCkThreads) {
             const int e = it / N, s = it % N;
-            halo[e * kCkMaxN + s] = cval(IN_PLANES, pl, e == 0 ? row0 : row0 + 65, s);
+            float2 v = f2(0.f, 0.f);
+            if (e == 0 && t > 0) v = __ldcg(my_edges - 2 * kCkMaxN + kCkMaxN + s);
+            if (e == 1 && t < p.mt - 1) v = __ldcg(my_edges + 2 * kCkMaxN + s);
+            halo[e * kCkMaxN + s] = v;
         }
+    };
+
+    // stencil weights of own row row0 + r for step (fwd1, j1) -> wts
+    auto fill_weights = [&](int r, bool ident, bool fwd1, int j1) {
+        const int yp = row0 + r, y = yp + 1;
+        float2 wc = f2(0.f, 0.f), wm = wc, wp = wc;
+        if (yp < n) {
+            if (ident) wc = f2(-1.f, 0.f);
+            else step_weights<ADJ>(p.co, fwd1, j1, y, wc, wm, wp);
+        }
+        wts[r] = wc;
+        wts[64 + r] = wm;
+        wts[128 + r] = wp;
     };
 
     // B of step k for this CTA's rows from the staged state:
@@ -236,7 +259,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
     // Exact H^H forward steps also write B into u(:, j-1) (stencil mode:
     // with its border rows).  Warp w handles sources w, w+8, ...; lane r the
     // rows 2r, 2r+1 (neighbour rows by shuffles).
-    auto produce = [&](int k, int mode, float *out) {
+    auto produce = [&](int k, int mode, float *out, bool wts_ready) {
         bool fwd1 = true;
         int j1 = nx;
         if (mode != P_TURN) j1 = col_of(k, fwd1);
@@ -245,72 +268,8 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         const bool wu = kind == K_EXACT && ADJ && fwd1 && !out;
         const bool has_base = (kind == K_EXACT || kind == K_LOCAL) && !ident;
         __syncthreads();
-        if (tid < 64) {
-            const int yp = row0 + tid, y = yp + 1;
-            float2 wc = f2(0.f, 0.f), wm = wc, wp = wc;
-            if (yp < n) {
-                if (ident) wc = f2(-1.f, 0.f);
-                else step_weights<ADJ>(p.co, fwd1, j1, y, wc, wm, wp);
-            }
-            wts[tid] = wc;
-            wts[64 + tid] = wm;
-            wts[128 + tid] = wp;
-        }
+        if (!wts_ready && tid < 64) fill_weights(tid, ident, fwd1, j1);
         __syncthreads();
-        const int yp0 = row0 + 2 * lane, y0 = yp0 + 1;
-        const bool v0 = yp0 < n, v1 = yp0 + 1 < n;
-        const bool in_k = yp0 < kCkRowsPerChunk * kc;
-        const float2 wc0 = wts[2 * lane], wm0 = wts[64 + 2 * lane], wp0 = wts[128 + 2 * lane];
-        const float2 wc1 = wts[2 * lane + 1], wm1 = wts[64 + 2 * lane + 1], wp1 = wts[128 + 2 * lane + 1];
-        for (int sb0 = warp; sb0 < N; sb0 += 4 * 8) {
-            float2 base[4][2];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int s = sb0 + 8 * q, gs = p.s0 + s;
-                base[q][0] = base[q][1] = f2(0.f, 0.f);
-                if (has_base && s < N && gs < p.s_end) {
-                    if (v0) base[q][0] = step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y0, gs);
-                    if (v1) base[q][1] = step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y0 + 1, gs);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int s = sb0 + 8 * q, gs = p.s0 + s;
-                if (s >= N) break;                                   // warp-uniform
-                const float4 cv = *reinterpret_cast<const float4 *>(cs + s * 64 + 2 * lane);
-                const float2 c0 = f2(cv.x, cv.y), c1 = f2(cv.z, cv.w);
-                float2 cm = f2(__shfl_up_sync(0xffffffffu, c1.x, 1), __shfl_up_sync(0xffffffffu, c1.y, 1));
-                float2 cp = f2(__shfl_down_sync(0xffffffffu, c0.x, 1), __shfl_down_sync(0xffffffffu, c0.y, 1));
-                if (lane == 0) cm = halo[s];
-                if (lane == 31) cp = halo[kCkMaxN + s];
-                float2 b0 = f2(0.f, 0.f), b1 = b0;
-                if (gs < p.s_end) {
-                    if (v0) {
-                        float2 acc = cmul(wc0, c0);
-                        cfma(acc, wm0, cm);
-                        cfma(acc, wp0, c1);
-                        b0 = csub(base[q][0], acc);
-                        if (wu) p.u[plane * gs + (size_t)ny * (j1 - 1) + y0] = b0;
-                    }
-                    if (v1) {
-                        float2 acc = cmul(wc1, c1);
-                        cfma(acc, wm1, c0);
-                        cfma(acc, wp1, cp);
-                        b1 = csub(base[q][1], acc);
-                        if (wu) p.u[plane * gs + (size_t)ny * (j1 - 1) + y0 + 1] = b1;
-                    }
-                }
-                if (out) {
-                    float *re = out + (size_t)s * ny, *im = out + (size_t)(kCkMaxN + s) * ny;
-                    if (v0 && gs < p.s_end) { __stcg(re + y0, b0.x); __stcg(im + y0, b0.y); }
-                    if (v1 && gs < p.s_end) { __stcg(re + y0 + 1, b1.x); __stcg(im + y0 + 1, b1.y); }
-                } else if (pack && in_k) {
-                    const int Q = yp0 / kCkRowsPerChunk, yl = yp0 % kCkRowsPerChunk;
-                    *reinterpret_cast<float4 *>(bg + (size_t)Q * bbytes + chunk_off(s, 2 * yl)) =
-                        make_float4(to_tf32(b0.x), to_tf32(b0.y), to_tf32(b1.x), to_tf32(b1.y));
-                }
-            }
-        }
         if (wu && !ident) {
             // border rows 0 and ny-1 of u(:, j1-1) (no B entry)
             for (int it = tid; it < 2 * N; it += kCkThreads) {
@@ -324,6 +283,82 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                 cfma(acc, wp, cs_get(yp + 1, s));
                 p.u[plane * gs + (size_t)ny * (j1 - 1) + y] =
                     csub(step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y, gs), acc);
+            }
+            __syncthreads();                               // the packing below overwrites the staged state
+        }
+        const int yp0 = row0 + 2 * lane, y0 = yp0 + 1;
+        const bool v0 = yp0 < n, v1 = yp0 + 1 < n;
+        const float2 wc0 = wts[2 * lane], wm0 = wts[64 + 2 * lane], wp0 = wts[128 + 2 * lane];
+        const float2 wc1 = wts[2 * lane + 1], wm1 = wts[64 + 2 * lane + 1], wp1 = wts[128 + 2 * lane + 1];
+        const int q_own = min(4, kc - row0 / kCkRowsPerChunk);    // packed chunks of this CTA's rows
+        // Warp: groups of 8 consecutive sources.  The packed chunks take the
+        // 8 sources of one row pair as one 128-byte row, so the warp writes
+        // its results over its own (already consumed) 4 KB of staged state in
+        // that order (XOR-swizzled against bank conflicts) and copies them out
+        // as contiguous 512-byte stores.
+        for (int grp = warp; grp < N / 8; grp += kCkWarps) {
+            float4 bq[8];
+#pragma unroll
+            for (int h4 = 0; h4 < 2; ++h4) {
+                float2 base[4][2];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int gs = p.s0 + 8 * grp + 4 * h4 + q;
+                    base[q][0] = base[q][1] = f2(0.f, 0.f);
+                    if (has_base && gs < p.s_end) {
+                        if (v0) base[q][0] = step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y0, gs);
+                        if (v1) base[q][1] = step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y0 + 1, gs);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int s = 8 * grp + 4 * h4 + q, gs = p.s0 + s;
+                    const float4 cv = *reinterpret_cast<const float4 *>(cs + s * 64 + 2 * lane);
+                    const float2 c0 = f2(cv.x, cv.y), c1 = f2(cv.z, cv.w);
+                    float2 cm = f2(__shfl_up_sync(0xffffffffu, c1.x, 1), __shfl_up_sync(0xffffffffu, c1.y, 1));
+                    float2 cp = f2(__shfl_down_sync(0xffffffffu, c0.x, 1), __shfl_down_sync(0xffffffffu, c0.y, 1));
+                    if (lane == 0) cm = halo[s];
+                    if (lane == 31) cp = halo[kCkMaxN + s];
+                    float2 b0 = f2(0.f, 0.f), b1 = b0;
+                    if (gs < p.s_end) {
+                        if (v0) {
+                            float2 acc = cmul(wc0, c0);
+                            cfma(acc, wm0, cm);
+                            cfma(acc, wp0, c1);
+                            b0 = csub(base[q][0], acc);
+                            if (wu) p.u[plane * gs + (size_t)ny * (j1 - 1) + y0] = b0;
+                        }
+                        if (v1) {
+                            float2 acc = cmul(wc1, c1);
+                            cfma(acc, wm1, c0);
+                            cfma(acc, wp1, cp);
+                            b1 = csub(base[q][1], acc);
+                            if (wu) p.u[plane * gs + (size_t)ny * (j1 - 1) + y0 + 1] = b1;
+                        }
+                        if (out) {
+                            float *re = out + (size_t)s * ny, *im = out + (size_t)(kCkMaxN + s) * ny;
+                            if (v0) { __stcg(re + y0, b0.x); __stcg(im + y0, b0.y); }
+                            if (v1) { __stcg(re + y0 + 1, b1.x); __stcg(im + y0 + 1, b1.y); }
+                        }
+                    }
+                    bq[4 * h4 + q] = make_float4(to_tf32(b0.x), to_tf32(b0.y), to_tf32(b1.x), to_tf32(b1.y));
+                }
+            }
+            if (pack) {
+                float4 *reg = reinterpret_cast<float4 *>(cs + (size_t)grp * 8 * 64);   // 256 float4
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < 8; ++q) reg[lane * 8 + (q ^ (lane & 7))] = bq[q];
+                __syncwarp();
+                for (int Q = 0; Q < q_own; ++Q) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int idx = lane + 32 * h, kg = idx >> 3;
+                        const float4 v = reg[(Q * 8 + kg) * 8 + ((idx & 7) ^ kg)];
+                        *reinterpret_cast<float4 *>(bg + (size_t)(row0 / kCkRowsPerChunk + Q) * bbytes +
+                                                    (size_t)grp * 1024 + (size_t)idx * 16) = v;
+                    }
+                }
             }
         }
     };
@@ -349,17 +384,17 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         const int part = l >> 6;                       // TMEM lanes 0-63: real parts, 64-127: imaginary
         const int row = l & 63;
         const bool row_ok = row0 + row < n;
-        const int hc = N / 2, c0 = (warp >> 2) * hc;
+        const int hc = ceil_div8(N / (kCkWarps / 4)), c0 = (warp >> 2) * hc;
         float *csf = reinterpret_cast<float *>(cs);
         const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
         int cb = 0;
-        for (; cb + 32 <= hc; cb += 32) {
+        for (; cb + 32 <= hc && c0 + cb + 32 <= N; cb += 32) {
             float v[32];
             tc::tmem_ld32(tl + (uint32_t)(c0 + cb), v);
 #pragma unroll
             for (int q = 0; q < 32; ++q) csf[((size_t)(c0 + cb + q) * 64 + row) * 2 + part] = row_ok ? v[q] : 0.f;
         }
-        for (; cb < hc; cb += 8) {
+        for (; cb < hc && c0 + cb < N; cb += 8) {
             float v[8];
             tc::tmem_ld8(tl + (uint32_t)(c0 + cb), v);
 #pragma unroll
@@ -379,11 +414,11 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         const int yp0 = row0 + 2 * lane, y0 = yp0 + 1;
         const bool v0 = yp0 < n, v1 = yp0 + 1 < n;
         __syncthreads();
-        for (int sb0 = warp; sb0 < N; sb0 += 4 * 8) {
+        for (int sb0 = warp; sb0 < N; sb0 += 4 * kCkWarps) {
             float2 o[4][2];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int s = sb0 + 8 * q, gs = p.s0 + s;
+                const int s = sb0 + kCkWarps * q, gs = p.s0 + s;
                 o[q][0] = o[q][1] = f2(0.f, 0.f);
                 if (s < N && gs < p.s_end) {
                     if (old_u) {
@@ -400,7 +435,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int s = sb0 + 8 * q, gs = p.s0 + s;
+                const int s = sb0 + kCkWarps * q, gs = p.s0 + s;
                 if (s >= N) break;                                   // warp-uniform
                 float4 *cp4 = reinterpret_cast<float4 *>(cs + s * 64 + 2 * lane);
                 float4 cv = *cp4;
@@ -416,9 +451,13 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                     if (v0) uc[y0] = f2(cv.x, cv.y);
                     if (v1) uc[y0 + 1] = f2(cv.z, cv.w);
                 }
-                float *re = curp + (size_t)s * ny, *im = curp + (size_t)(kCkMaxN + s) * ny;
-                if (v0 && (last || lane == 0)) { __stcg(re + y0, cv.x); __stcg(im + y0, cv.y); }
-                if (v1 && (last || lane == 31)) { __stcg(re + y0 + 1, cv.z); __stcg(im + y0 + 1, cv.w); }
+                if (lane == 0) __stcg(my_edges + s, f2(cv.x, cv.y));
+                if (lane == 31 && v1) __stcg(my_edges + kCkMaxN + s, f2(cv.z, cv.w));
+                if (last) {
+                    float *re = curp + (size_t)s * ny, *im = curp + (size_t)(kCkMaxN + s) * ny;
+                    if (v0) { __stcg(re + y0, cv.x); __stcg(im + y0, cv.y); }
+                    if (v1) { __stcg(re + y0 + 1, cv.z); __stcg(im + y0 + 1, cv.w); }
+                }
             }
         }
         if (kind == K_EXACT && ADJ && !fwd && t == 0) {
@@ -507,7 +546,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
             mode0 = P_IDENT;                               // first B = 0
         }
         stage_in(in0, pl0);
-        produce(0, mode0, nullptr);
+        produce(0, mode0, nullptr, false);
         epoch += (unsigned)p.mt;
         ok = counter_sync(ctr, epoch, p.err, s_ok, p.timeout_ns, SITE_B);
     }
@@ -559,6 +598,14 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
             if (!good) atomicCAS(p.err, 0, SITE_COPY);
         }
         if (warp >= 1) prefetch_cols(k);
+        if (warp == 1 || warp == 2) {
+            const bool next_b = k + 1 < nsteps || (ADJ && p.pass == CK_FIRST && chunk + 1 < p.C);
+            if (next_b) {
+                bool f1 = false;
+                const int j1 = col_of(k + 1, f1);
+                fill_weights(tid - 32, kind == K_BOUND, f1, j1);
+            }
+        }
         CPROF(0);
         if (!tc::mbar_wait(done, (uint32_t)(k & 1), p.timeout_ns)) atomicCAS(p.err, 0, SITE_MMA);
         tc::fence_after();
@@ -582,8 +629,9 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         tc::fence_after();
         CPROF(3);
         if (k + 1 < nsteps) {
-            stage_halo(curp);
-            produce(k + 1, kind == K_BOUND ? P_IDENT : P_STENCIL, nullptr);
+            stage_halo();
+            CPROF(5);
+            produce(k + 1, kind == K_BOUND ? P_IDENT : P_STENCIL, nullptr, true);
             CPROF(4);
             epoch += (unsigned)p.mt;
             if (!counter_sync(ctr, epoch, p.err, s_ok, p.timeout_ns, SITE_B)) {
@@ -591,12 +639,12 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                 break;
             }
         } else if (kind == K_EXACT && ADJ && p.half == 0 && t0 + k == nx - 2) {
-            stage_halo(curp);
-            produce(k, P_TURN, nullptr);
+            stage_halo();
+            produce(k, P_TURN, nullptr, false);
         } else if (ADJ && p.pass == CK_FIRST && chunk + 1 < p.C) {
             // outgoing B state of the chunk: the first B of the next chunk
-            stage_halo(curp);
-            produce(k + 1, P_STENCIL, bstate(chunk));
+            stage_halo();
+            produce(k + 1, P_STENCIL, bstate(chunk), true);
         }
     }
 
@@ -700,6 +748,7 @@ static ChunkParams base_params(const Coefs<float2> &co, const TcChunkGeom &g, co
     p.bglob = b.bglob;
     p.zst = b.zst;
     p.sb = b.sb;
+    p.edges = b.edges;
     p.group_ctr = b.sync;
     p.err = b.err;
     p.ny = co.ny;
