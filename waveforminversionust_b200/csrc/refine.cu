@@ -15,104 +15,110 @@
 
 namespace wust {
 
-constexpr int kResThreads = 128;
-constexpr int kResMaxS = 1024;          // per-block source norms kept in shared memory
+constexpr int kResRows = 128;          // grid rows per block (one per thread)
+constexpr int kResSrc = 8;             // sources per thread
+constexpr int kResCols = 16;           // columns per block
 
-// One thread per grid point (y, x): its nine coefficients (or their
-// conjugates for H^H) are loaded once and reused for every source.
+// One thread per grid row y of a block's 16 columns and 8 sources: the nine
+// coefficients (or their conjugates for H^H) of a point are loaded once and
+// reused for the 8 sources; walking the columns keeps the neighbour columns'
+// lines in L1; the per-source norms accumulate in registers and are reduced
+// once per warp at the end.
 template <bool ADJ>
-__global__ void __launch_bounds__(kResThreads) residual_kernel(Coefs<double2> co, SrcView b, const double2 *x, int S,
-                                                               float2 *r32, double *rnorm2, double *bnorm2) {
-    __shared__ double srr[kResMaxS], sbb[kResMaxS];
+__global__ void __launch_bounds__(kResRows) residual_kernel(Coefs<double2> co, SrcView b, const double2 *__restrict__ x,
+                                                            int S, float2 *r32, double *rnorm2, double *bnorm2) {
     const int ny = co.ny, nx = co.nx;
-    const int y = blockIdx.x * blockDim.x + threadIdx.x;
-    const int xi = blockIdx.y;
-    for (int s = threadIdx.x; s < S; s += blockDim.x) { srr[s] = 0.0; sbb[s] = 0.0; }
-    __syncthreads();
-    const bool active = (y >= 1 && y <= ny - 2 && xi < nx);
-    // stencil taps: neighbour offsets (dy, dx) and coefficients
-    double2 w[9];
-    int dyv[9], dxv[9];
-    const double2 z = make_double2(0.0, 0.0);
-    if (active) {
-        const bool xl = xi >= 1, xr = xi <= nx - 2;
-        if (!ADJ) {
-            w[0] = co.dd(y, xi);               dyv[0] = 0;  dxv[0] = 0;
-            w[1] = co.dl(y - 1, xi);           dyv[1] = -1; dxv[1] = 0;
-            w[2] = co.du(y, xi);               dyv[2] = 1;  dxv[2] = 0;
-            w[3] = xl ? co.ld(y, xi - 1) : z;      dyv[3] = 0;  dxv[3] = -1;
-            w[4] = xl ? co.ll(y - 1, xi - 1) : z;  dyv[4] = -1; dxv[4] = -1;
-            w[5] = xl ? co.lu(y, xi - 1) : z;      dyv[5] = 1;  dxv[5] = -1;
-            w[6] = xr ? co.ud(y, xi) : z;          dyv[6] = 0;  dxv[6] = 1;
-            w[7] = xr ? co.ul(y - 1, xi) : z;      dyv[7] = -1; dxv[7] = 1;
-            w[8] = xr ? co.uu(y, xi) : z;          dyv[8] = 1;  dxv[8] = 1;
-        } else {
-            w[0] = zconj(co.dd(y, xi));            dyv[0] = 0;  dxv[0] = 0;
-            w[1] = zconj(co.dl(y, xi));            dyv[1] = 1;  dxv[1] = 0;
-            w[2] = zconj(co.du(y - 1, xi));        dyv[2] = -1; dxv[2] = 0;
-            w[3] = xr ? zconj(co.ld(y, xi)) : z;          dyv[3] = 0;  dxv[3] = 1;
-            w[4] = xr ? zconj(co.ll(y, xi)) : z;          dyv[4] = 1;  dxv[4] = 1;
-            w[5] = xr ? zconj(co.lu(y - 1, xi)) : z;      dyv[5] = -1; dxv[5] = 1;
-            w[6] = xl ? zconj(co.ud(y, xi - 1)) : z;      dyv[6] = 0;  dxv[6] = -1;
-            w[7] = xl ? zconj(co.ul(y, xi - 1)) : z;      dyv[7] = 1;  dxv[7] = -1;
-            w[8] = xl ? zconj(co.uu(y - 1, xi - 1)) : z;  dyv[8] = -1; dxv[8] = -1;
-        }
-        // taps that leave the grid have zero weight; clamp their index
-#pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            const int xx = xi + dxv[t];
-            if (xx < 0 || xx >= nx) { dxv[t] = 0; w[t] = z; }
-        }
-    }
+    const int y = blockIdx.x * kResRows + threadIdx.x;
+    const int s0 = blockIdx.y * kResSrc;
+    const int x0 = blockIdx.z * kResCols, x1 = min(nx, x0 + kResCols);
+    const bool active = (y >= 1 && y <= ny - 2);
     const size_t plane = (size_t)ny * nx;
-    const size_t me = (size_t)y + (size_t)ny * xi;
-    for (int s = 0; s < S; ++s) {
-        double rr = 0, bb = 0;
-        if (y < ny && xi < nx) {
+    const double2 z = make_double2(0.0, 0.0);
+    double rr[kResSrc], bb[kResSrc];
+#pragma unroll
+    for (int q = 0; q < kResSrc; ++q) { rr[q] = 0.0; bb[q] = 0.0; }
+    for (int xi = x0; xi < x1; ++xi) {
+        // stencil taps: neighbour offsets (dy, dx) and coefficients
+        double2 w[9];
+        int dyv[9], dxv[9];
+        if (active) {
+            const bool xl = xi >= 1, xr = xi <= nx - 2;
+            if (!ADJ) {
+                w[0] = co.dd(y, xi);               dyv[0] = 0;  dxv[0] = 0;
+                w[1] = co.dl(y - 1, xi);           dyv[1] = -1; dxv[1] = 0;
+                w[2] = co.du(y, xi);               dyv[2] = 1;  dxv[2] = 0;
+                w[3] = xl ? co.ld(y, xi - 1) : z;      dyv[3] = 0;  dxv[3] = -1;
+                w[4] = xl ? co.ll(y - 1, xi - 1) : z;  dyv[4] = -1; dxv[4] = -1;
+                w[5] = xl ? co.lu(y, xi - 1) : z;      dyv[5] = 1;  dxv[5] = -1;
+                w[6] = xr ? co.ud(y, xi) : z;          dyv[6] = 0;  dxv[6] = 1;
+                w[7] = xr ? co.ul(y - 1, xi) : z;      dyv[7] = -1; dxv[7] = 1;
+                w[8] = xr ? co.uu(y, xi) : z;          dyv[8] = 1;  dxv[8] = 1;
+            } else {
+                w[0] = zconj(co.dd(y, xi));            dyv[0] = 0;  dxv[0] = 0;
+                w[1] = zconj(co.dl(y, xi));            dyv[1] = 1;  dxv[1] = 0;
+                w[2] = zconj(co.du(y - 1, xi));        dyv[2] = -1; dxv[2] = 0;
+                w[3] = xr ? zconj(co.ld(y, xi)) : z;          dyv[3] = 0;  dxv[3] = 1;
+                w[4] = xr ? zconj(co.ll(y, xi)) : z;          dyv[4] = 1;  dxv[4] = 1;
+                w[5] = xr ? zconj(co.lu(y - 1, xi)) : z;      dyv[5] = -1; dxv[5] = 1;
+                w[6] = xl ? zconj(co.ud(y, xi - 1)) : z;      dyv[6] = 0;  dxv[6] = -1;
+                w[7] = xl ? zconj(co.ul(y, xi - 1)) : z;      dyv[7] = 1;  dxv[7] = -1;
+                w[8] = xl ? zconj(co.uu(y - 1, xi - 1)) : z;  dyv[8] = -1; dxv[8] = -1;
+            }
+            // taps that leave the grid have zero weight; clamp their index
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                const int xx = xi + dxv[t];
+                if (xx < 0 || xx >= nx) { dxv[t] = 0; w[t] = z; }
+            }
+        }
+        const size_t me = (size_t)y + (size_t)ny * xi;
+        const bool interior = xi > 0 && xi < nx - 1;    // norms over the interior grid (see accumulate_kernel)
+#pragma unroll
+        for (int q = 0; q < kResSrc; ++q) {
+            const int s = s0 + q;
+            if (s >= S || y >= ny) continue;
             double2 r = z;
             if (active) {
                 const double2 *xs = x + plane * s;
                 double2 h = z;
 #pragma unroll
                 for (int t = 0; t < 9; ++t) {
-                    const double2 v = xs[(size_t)(y + dyv[t]) + (size_t)ny * (xi + dxv[t])];
+                    const double2 v = __ldg(xs + (size_t)(y + dyv[t]) + (size_t)ny * (xi + dxv[t]));
                     h.x += w[t].x * v.x - w[t].y * v.y;
                     h.y += w[t].x * v.y + w[t].y * v.x;
                 }
                 const double2 bv = z_from(b.get(y, xi, s, ny, nx));
                 r = zsub(bv, h);
-                if (xi > 0 && xi < nx - 1) {        // norms over the interior grid (see accumulate_kernel)
-                    rr = zabs2(r);
-                    bb = zabs2(bv);
+                if (interior) {
+                    rr[q] += zabs2(r);
+                    bb[q] += zabs2(bv);
                 }
             }
             r32[plane * s + me] = c_from(r);
         }
+    }
+#pragma unroll
+    for (int q = 0; q < kResSrc; ++q) {
+        double a = rr[q], c = bb[q];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            rr += __shfl_xor_sync(0xffffffffu, rr, o);
-            bb += __shfl_xor_sync(0xffffffffu, bb, o);
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            c += __shfl_xor_sync(0xffffffffu, c, o);
         }
-        if ((threadIdx.x & 31) == 0 && (rr != 0 || bb != 0)) {
-            atomicAdd(&srr[s], rr);
-            atomicAdd(&sbb[s], bb);
+        if ((threadIdx.x & 31) == 0 && s0 + q < S) {
+            if (a != 0) atomicAdd(&rnorm2[s0 + q], a);
+            if (bnorm2 && c != 0) atomicAdd(&bnorm2[s0 + q], c);
         }
-    }
-    __syncthreads();
-    for (int s = threadIdx.x; s < S; s += blockDim.x) {
-        if (srr[s] != 0) atomicAdd(&rnorm2[s], srr[s]);
-        if (bnorm2 && sbb[s] != 0) atomicAdd(&bnorm2[s], sbb[s]);
     }
 }
 
 void residual_launch(const Coefs<double2> &co, const SrcView &b, const double2 *x, int S, bool adjoint, float2 *r32,
                      double *rnorm2, double *bnorm2, cudaStream_t st) {
-    if (S > kResMaxS) fail(WUST_ERR_INVALID_INPUT, "refined solves support at most %d sources per batch", kResMaxS);
     WUST_CUDA(cudaMemsetAsync(rnorm2, 0, sizeof(double) * S, st));
     if (bnorm2) WUST_CUDA(cudaMemsetAsync(bnorm2, 0, sizeof(double) * S, st));
-    dim3 grid(ceil_div(co.ny, kResThreads), co.nx);
-    if (adjoint) residual_kernel<true><<<grid, kResThreads, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
-    else residual_kernel<false><<<grid, kResThreads, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
+    dim3 grid(ceil_div(co.ny, kResRows), ceil_div(S, kResSrc), ceil_div(co.nx, kResCols));
+    if (adjoint) residual_kernel<true><<<grid, kResRows, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
+    else residual_kernel<false><<<grid, kResRows, 0, st>>>(co, b, x, S, r32, rnorm2, bnorm2);
     ++g_kernel_launches;
     WUST_LAUNCH_CHECK();
 }
