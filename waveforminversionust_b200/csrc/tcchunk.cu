@@ -504,13 +504,17 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
 
     // ---- bulk-copy ring (thread 0); chunk ci = k * kc + q of step k --------
     uint32_t a_next = 0, b_next = 0, retired = 0, full_waited = 0;
+    // the page stream passes through L2 once; the packed B is read by every
+    // CTA of the group and should stay
+    const uint64_t a_policy = tc::policy_evict_first();
+    const uint64_t b_policy = tc::policy_evict_last();
     auto pump = [&](int k, bool b_ready) {
         const uint32_t a_end = (uint32_t)min(k + 2, nsteps) * (uint32_t)kc;
         while (a_next < a_end && a_next < retired + kCkStages) {
             const int ks = (int)(a_next / kc), q = (int)(a_next % kc), slot = (int)(a_next % kCkStages);
             tc::mbar_expect_tx(&full[slot], tc::kAChunk);
-            tc::bulk_g2s(sA + (size_t)slot * tc::kAChunk, apage(ks) + ((size_t)t * kc + q) * tc::kAChunk, tc::kAChunk,
-                         &full[slot]);
+            tc::bulk_g2s_hint(sA + (size_t)slot * tc::kAChunk, apage(ks) + ((size_t)t * kc + q) * tc::kAChunk,
+                              tc::kAChunk, &full[slot], a_policy);
             ++a_next;
         }
         if (b_ready) {
@@ -518,7 +522,8 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
             while (b_next < b_end && b_next < a_next) {
                 const int q = (int)(b_next % kc), slot = (int)(b_next % kCkStages);
                 tc::mbar_expect_tx(&full[slot], (uint32_t)bbytes);
-                tc::bulk_g2s(sB + (size_t)slot * kCkBSlot, bg + (size_t)q * bbytes, (uint32_t)bbytes, &full[slot]);
+                tc::bulk_g2s_hint(sB + (size_t)slot * kCkBSlot, bg + (size_t)q * bbytes, (uint32_t)bbytes, &full[slot],
+                                  b_policy);
                 ++b_next;
             }
         }
