@@ -47,7 +47,8 @@ constexpr int NTN = 112;                           // MMA N: complex columns per
 constexpr int kRows = 64;                          // complex rows per M tile
 constexpr int kKRows = 16;                         // complex K rows per chunk
 constexpr int kStages = 7;
-constexpr int kNsThreads = 256;
+constexpr int kNsThreads = 512;
+constexpr int kPartCols = (NTN / (kNsThreads / 128) + 7) / 8 * 8;   // TMEM columns per warp of the partial tile
 constexpr int kBChunkNs = NTN * tc::kChunkBytes;   // 14 KB
 constexpr int kStageBytes = tc::kAChunk + kBChunkNs;
 constexpr size_t kNsSmem = (size_t)kStages * kStageBytes + 512;
@@ -231,12 +232,14 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         NSPROF(2);
         ++n_gemm;
         tc::fence_after();
-        // partial tile: warp w reads TMEM lanes 32(w%4).., columns half (w/4)
+        // partial tile: warp w reads TMEM lanes 32(w%4).., columns
+        // [kPartCols (w/4), kPartCols (w/4 + 1)) within the tile
         const int row = 32 * (warp & 3) + lane;
-        const int cb0 = (NTN / 2) * (warp >> 2);
+        const int cb0 = kPartCols * (warp >> 2);
         float *mypart = p.part + ((size_t)(tile * KS + ks) * 128 + row) * NTN + cb0;
 #pragma unroll
-        for (int cb = 0; cb < NTN / 2; cb += 8) {
+        for (int cb = 0; cb < kPartCols; cb += 8) {
+            if (cb0 + cb >= NTN) break;                // warp-uniform
             float t[8];
             if (nch > 0) {
                 tc::tmem_ld8(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(cb0 + cb), t);
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     // Rows of this tile whose split-K sum this CTA forms.
     const int rows_per = ((kRows + KS - 1) / KS + 1) & ~1;   // even: B-layout units hold row pairs
     const int rbeg = ks * rows_per, rend = min(kRows, rbeg + rows_per);
-    // This CTA's epilogue items: item m of thread tid is it = tid + 256 m over
+    // This CTA's epilogue items: item m of thread tid is it = tid + kNsThreads m over
     // the (rend - rbeg) x NTN slice; their split-K sums, with every load of a
     // rank in flight at once.
     constexpr int kEpi = ((kRows + 2) / 3 * NTN + kNsThreads - 1) / kNsThreads;   // bound for ks >= 3
