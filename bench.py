@@ -395,10 +395,10 @@ def main():
                  if args.precision == "tf32-refined" else "factor_kernel (Schur recursion + Gauss-Jordan inverses)")
     # DRAM bytes of one sweep pair of the dominant kernel (its six launches),
     # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one
-    # pass) at 552^2 with 256 sources: 13.61 GB read + 2.74 GB written
+    # pass) at 552^2 with 256 sources: 12.48 GB read + 1.18 GB written
     traffic = None
     if flop == fl["apply"] and args.precision == "tf32-refined" and WORKLOAD == "config2":
-        traffic = 16.34e9
+        traffic = 13.66e9
     roofline = dict(kernel=kname, bound="tensor", achieved=achieved, peak=peak_tf, unit="TFLOP/s",
                     frac=achieved / peak_tf, peak_source=peak_src, traffic=traffic,
                     traffic_unit="bytes per launch (ncu)", hbm_gbs_achieved=(
