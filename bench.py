@@ -206,6 +206,44 @@ def generate_observations(p, solver_cls, torch):
     return Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, [FREQ], Y, mask)
 
 
+def run_ncg(args, p, obs, torch):
+    """NCG updates of wust_reconstruct (oracle + ROI/filter + direction +
+    curvature + step + projection) at the workload's frequency, with the
+    update rules on the device (the library's wust_ncg_* entry points) and on
+    the host (NumPy, as the reference runs them in MATLAB)."""
+    from waveforminversionust_b200.objective import POOL
+    from waveforminversionust_b200.reconstruct import wust_reconstruct
+    ny, nx = p.shape
+    mask = np.zeros((ny, nx))
+    mask[20:-20, 20:-20] = 1.0
+    n = args.warmup + args.steps
+    cfg = dict(backend="gpu", bounds_mps=(1300.0, 1800.0), max_update_mps=10.0, step_damping=1.0,
+               source_batch_size=N_TX, pml_strength=10.0, pml_m=p.pml_m, stencil_bounds=(1400.0, 1700.0),
+               wavenumber="continuum", filter_cutoff=0.75, filter_order=4, update_mask=mask,
+               frequency_schedule_hz=[FREQ] * n, precision=args.precision)
+    res = {}
+    for dev in (True, False):
+        POOL.clear()
+        torch.cuda.synchronize()
+        out = wust_reconstruct(obs, p.c_init, dict(cfg, ncg_device=dev))
+        recs = out["records"][args.warmup:]
+        res[dev] = dict(ms_per_update=1e3 * float(np.mean([r["wall_seconds"] for r in recs])),
+                        curvature_ms=1e3 * float(np.mean([r["linearized_seconds"] for r in recs])),
+                        loss_first=out["records"][0]["loss_before_update"],
+                        loss_last=out["records"][-1]["loss_before_update"])
+    POOL.clear()
+    dev, host = res[True], res[False]
+    print(json.dumps(dict(
+        metric="ncg_updates_per_second", value=1e3 / dev["ms_per_update"], unit="updates/s", n_gpus=1,
+        steps=args.steps, warmup=args.warmup, ms_per_step=dev["ms_per_update"], higher_is_better=True,
+        scaling="weak", vs_baseline=None, dtype="tf32+c128-refine" if args.precision == "tf32-refined" else args.precision,
+        data="synthetic",
+        config=dict(workload=WORKLOADS[WORKLOAD]["text"], loop="wust_reconstruct NCG update, one frequency",
+                    filter_cutoff=0.75, precision=args.precision, timing="host wall clock per update"),
+        host_rules=dict(value=1e3 / host["ms_per_update"], ms_per_update=host["ms_per_update"]),
+        detail=dict(device=dev, host=host))))
+
+
 def run_solves(args, p, solver_cls, torch):
     """Factor once, then time forward solves of all transmitters (one line of JSON)."""
     ny, nx = p.shape
@@ -243,8 +281,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="c64,c64-refined", help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve"],
-                    help="solve: factor once, then time forward solves of all transmitters (kernel profiling)")
+    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg"],
+                    help="solve: factor once, then time forward solves of all transmitters (kernel profiling); "
+                         "ncg: time NCG updates of the reconstruction loop, update rules on the device and on the host")
     args = ap.parse_args()
     global WORKLOAD, N_TX, FREQ
     WORKLOAD = args.workload
@@ -276,6 +315,9 @@ def main():
         run_solves(args, p, HelmholtzSolver, torch)
         return
     obs = generate_observations(p, HelmholtzSolver, torch)
+    if args.mode == "ncg":
+        run_ncg(args, p, obs, torch)
+        return
     fl = flops_per_gradient(ny, nx, N_TX)
     stream = torch.cuda.current_stream()
 

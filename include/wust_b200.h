@@ -205,6 +205,31 @@ int wust_solver_oracle(wust_solver *s, const int32_t *tx_index, int n_tx,
  * (directional_curvature.m:1-26).  direction: ny x nx double. */
 int wust_solver_curvature(wust_solver *s, const double *direction, double *curvature);
 
+/* The NCG update of wust_reconstruct (wust_reconstruct.m:24-57) on the GPU,
+ * FP64, for hosts that keep the model, gradient and direction in device
+ * memory between oracle calls (the reference runs these rules in MATLAB on
+ * the host).  Every field is a device pointer to ny x nx column-major doubles
+ * on the solver's grid; update masks are device bytes (0/1).  Calls are
+ * ordered on the solver's stream; scalar outputs synchronize it. */
+
+/* roi = M g; z = M F M g with F the ringing filter (wust_roi_gradient.m:1-10,
+ * ringingRemovalFilt.m:1-45, FFT by cuFFT; cutoff 0: z = roi).  c0: the
+ * reference speed the filter cutoff is scaled with (the mean initial speed). */
+int wust_ncg_roi_gradient(wust_solver *s, const double *gradient, const uint8_t *update_mask, double c0,
+                          double frequency_hz, double cutoff, double order, double *roi, double *z);
+/* Clipped PR/FR direction with restart on non-descent (wust_ncg_direction.m:1-17).
+ * direction: the previous direction on input, the new one on output. */
+int wust_ncg_direction(wust_solver *s, const double *roi, const double *z, const double *prev_z, double prev_gz,
+                       int same_frequency, double *direction, double *beta, double *gz);
+/* sum a .* b over the grid (the directional slope roi' * direction). */
+int wust_ncg_dot(wust_solver *s, const double *a, const double *b, double *out);
+/* c <- projected update of the slowness 1/c + step_damping * alpha * direction
+ * (wust_project_slowness_update.m:1-10); relative_update (nullable) receives
+ * ||1/c_new - 1/c_old|| / ||1/c_old|| over the mask (wust_reconstruct.m:56). */
+int wust_ncg_project(wust_solver *s, double *c, const double *direction, double alpha, double step_damping,
+                     double max_update_mps, double c_min, double c_max, const uint8_t *update_mask,
+                     double *relative_update);
+
 /* Counters of the last solve/oracle call: correction solves of the last
  * refined solve, its final relative FP64 residual |b - Hx| / |b| and forward
  * error estimate (refined profiles; -1 otherwise), and the number of kernel

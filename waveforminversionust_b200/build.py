@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwust_b200.so")
-SOURCES = ["api.cu", "assemble.cu", "factor.cu", "sweep.cu", "objective.cu", "refine.cu", "noalloc.cu", "tcsweep.cu", "tcchunk.cu", "nsfactor.cu"]
+SOURCES = ["api.cu", "assemble.cu", "factor.cu", "sweep.cu", "objective.cu", "refine.cu", "noalloc.cu", "tcsweep.cu", "tcchunk.cu", "nsfactor.cu", "ncg.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -55,7 +55,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-Xcompiler", "-fPIC"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-Xcompiler", "-fPIC", "-lcufft"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

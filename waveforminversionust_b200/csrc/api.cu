@@ -1,11 +1,14 @@
 // C ABI of libwust_b200: the HelmholtzSolver object, the two legacy
 // MEX-equivalent entry points and the oracle/curvature drivers.
 #include <cmath>
+#include <limits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
+
+#include <cufft.h>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -94,6 +97,12 @@ struct wust_solver {
     double refine_tol = 1e-5;
     int factor_method = WUST_FACTOR_DEFAULT;
     int sweep_method = WUST_SWEEP_DEFAULT;
+    // NCG update on the device: real 2-D FFT plans of the grid, half spectrum,
+    // block partials of the reductions (created on first use)
+    bool fft_ready = false;
+    cufftHandle fft_fwd = 0, fft_inv = 0;
+    double2 *spec = nullptr;
+    double *ncg_part = nullptr;
     double f = 0, sgn = -1, a0 = 0, L = 0, vmin = 0, vmax = 0;
     int ldr9 = 0;
     double dt = 0, cr = 0;
@@ -201,6 +210,12 @@ static void free_solver(wust_solver *s) {
                     s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err, s->ns_scratch,
                     s->ck_lpack, s->ck_b, s->ck_z, s->ck_sb, s->ck_edges, s->ck_sync};
     for (void *p : ptrs) dfree(p);
+    if (s->fft_ready) {
+        cufftDestroy(s->fft_fwd);
+        cufftDestroy(s->fft_inv);
+    }
+    dfree(s->spec);
+    dfree(s->ncg_part);
     for (int i = 0; i < 9; ++i) { dfree(s->c128[i]); dfree(s->c64[i]); }
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
     for (auto &e : s->sw_ev) if (e) cudaEventDestroy(e);
@@ -865,6 +880,113 @@ int wust_solver_curvature(wust_solver *s, const double *direction, double *curva
         if (!std::isfinite(k)) fail(WUST_ERR_NUMERICAL_FAILURE, "Nonfinite curvature");
         *curvature = k;
         s->launches = g_kernel_launches - t0;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// NCG update on the device (wust_reconstruct.m:24-57)
+// ---------------------------------------------------------------------------
+static double *ncg_partials(wust_solver *s) {
+    if (!s->ncg_part) s->ncg_part = dalloc<double>(3 * (size_t)kNcgMaxBlocks);
+    return s->ncg_part;
+}
+// Sum `per` values over nb block partials, in block order.
+static std::vector<double> ncg_sum(wust_solver *s, int nb, int per) {
+    std::vector<double> h((size_t)nb * per), out(per, 0.0);
+    WUST_CUDA(cudaMemcpyAsync(h.data(), s->ncg_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    WUST_CUDA(cudaStreamSynchronize(s->st));
+    for (int b = 0; b < nb; ++b)
+        for (int k = 0; k < per; ++k) out[k] += h[(size_t)b * per + k];
+    return out;
+}
+static double mean_step(const std::vector<double> &v) {
+    double t = 0;
+    for (size_t i = 1; i < v.size(); ++i) t += v[i] - v[i - 1];
+    return t / (double)(v.size() - 1);
+}
+static void check_cufft(cufftResult r, const char *what) {
+    if (r != CUFFT_SUCCESS) fail(WUST_ERR_CUDA, "%s failed (cufft %d)", what, (int)r);
+}
+
+int wust_ncg_roi_gradient(wust_solver *s, const double *gradient, const uint8_t *update_mask, double c0,
+                          double frequency_hz, double cutoff, double order, double *roi, double *z) {
+    return guarded([&] {
+        if (!s || !gradient || !update_mask || !roi || !z) fail(WUST_ERR_INVALID_INPUT, "roi_gradient arguments missing");
+        if (!(std::isfinite(cutoff) && cutoff >= 0)) fail(WUST_ERR_INVALID_INPUT, "cutoff must be a finite nonnegative scalar");
+        if (cutoff > 0 && !(std::isfinite(order) && order > 0 && std::isfinite(c0) && c0 > 0 && frequency_hz > 0))
+            fail(WUST_ERR_INVALID_INPUT, "filter order, speed and frequency must be positive and finite");
+        const long long t0 = g_kernel_launches;
+        const size_t N = s->plane();
+        cudaStream_t st = s->st;
+        ncg_roi_launch(gradient, update_mask, roi, N, st);
+        if (cutoff == 0) {
+            WUST_CUDA(cudaMemcpyAsync(z, roi, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        } else {
+            if (!s->fft_ready) {
+                // column-major ny x nx = row-major (nx, ny): half spectrum along y
+                check_cufft(cufftPlan2d(&s->fft_fwd, s->nx, s->ny, CUFFT_D2Z), "cufftPlan2d");
+                check_cufft(cufftPlan2d(&s->fft_inv, s->nx, s->ny, CUFFT_Z2D), "cufftPlan2d");
+                s->spec = dalloc<double2>((size_t)s->nx * (s->ny / 2 + 1));
+                s->fft_ready = true;
+            }
+            check_cufft(cufftSetStream(s->fft_fwd, st), "cufftSetStream");
+            check_cufft(cufftSetStream(s->fft_inv, st), "cufftSetStream");
+            check_cufft(cufftExecD2Z(s->fft_fwd, roi, reinterpret_cast<cufftDoubleComplex *>(s->spec)), "cufftExecD2Z");
+            const double kc = (2.0 * frequency_hz / c0) * cutoff;
+            ncg_butterworth_launch(s->spec, s->nx, s->ny, mean_step(s->xs), mean_step(s->ys), kc * kc, order, st);
+            check_cufft(cufftExecZ2D(s->fft_inv, reinterpret_cast<cufftDoubleComplex *>(s->spec), z), "cufftExecZ2D");
+            ncg_mask_scale_launch(z, update_mask, 1.0 / ((double)s->nx * s->ny), N, st);
+        }
+        s->launches = g_kernel_launches - t0;
+    });
+}
+
+int wust_ncg_direction(wust_solver *s, const double *roi, const double *z, const double *prev_z, double prev_gz,
+                       int same_frequency, double *direction, double *beta_out, double *gz_out) {
+    return guarded([&] {
+        if (!s || !roi || !z || !prev_z || !direction || !beta_out || !gz_out)
+            fail(WUST_ERR_INVALID_INPUT, "ncg_direction arguments missing");
+        const size_t N = s->plane();
+        double *part = ncg_partials(s);
+        const std::vector<double> d2 = ncg_sum(s, ncg_dot2_launch(roi, z, prev_z, N, part, s->st), 2);
+        const double gz = d2[0];
+        double beta = 0.0;
+        if (same_frequency && prev_gz > 0) {
+            const double beta_fr = gz / prev_gz, beta_pr = d2[1] / prev_gz;
+            beta = std::min(std::max(beta_pr, 0.0), beta_fr);
+        }
+        std::vector<double> dd = ncg_sum(s, ncg_direction_launch(z, roi, beta, direction, N, part, s->st), 2);
+        if (dd[0] >= 0) {                         // not a descent direction: restart with -z
+            beta = 0.0;
+            dd = ncg_sum(s, ncg_direction_launch(z, roi, 0.0, direction, N, part, s->st), 2);
+        }
+        if (dd[1] != 0 || !std::isfinite(gz) || gz < 0)
+            fail(WUST_ERR_NUMERICAL_FAILURE, "Invalid preconditioned gradient");
+        *beta_out = beta;
+        *gz_out = gz;
+    });
+}
+
+int wust_ncg_dot(wust_solver *s, const double *a, const double *b, double *out) {
+    return guarded([&] {
+        if (!s || !a || !b || !out) fail(WUST_ERR_INVALID_INPUT, "ncg_dot arguments missing");
+        *out = ncg_sum(s, ncg_dot_launch(a, b, s->plane(), ncg_partials(s), s->st), 1)[0];
+    });
+}
+
+int wust_ncg_project(wust_solver *s, double *c, const double *direction, double alpha, double step_damping,
+                     double max_update_mps, double c_min, double c_max, const uint8_t *update_mask,
+                     double *relative_update) {
+    return guarded([&] {
+        if (!s || !c || !direction || !update_mask) fail(WUST_ERR_INVALID_INPUT, "ncg_project arguments missing");
+        if (!(c_min > 0 && c_max > c_min && max_update_mps > 0 && step_damping > 0 && std::isfinite(alpha)))
+            fail(WUST_ERR_INVALID_INPUT, "Invalid speed bounds or step");
+        const std::vector<double> r = ncg_sum(
+            s, ncg_project_launch(c, direction, step_damping * alpha, max_update_mps, c_min, c_max, update_mask,
+                                  s->plane(), ncg_partials(s), s->st), 3);
+        if (r[0] != 0) fail(WUST_ERR_NUMERICAL_FAILURE, "Nonfinite slowness trial");
+        if (relative_update)
+            *relative_update = std::sqrt(r[1]) / std::max(std::sqrt(r[2]), std::numeric_limits<double>::min());
     });
 }
 

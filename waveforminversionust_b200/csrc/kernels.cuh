@@ -78,6 +78,20 @@ void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_
 void tc_chunk_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
                     const TcChunkBuffers &b, const SrcView &src, int S, bool adjoint, float2 *u, cudaStream_t st);
 
+// ---- ncg.cu (NCG update, FP64) -------------------------------------------------
+constexpr int kNcgMaxBlocks = 592;    // partials per reduction (<= 3 values each)
+void ncg_roi_launch(const double *g, const uint8_t *mask, double *roi, size_t n, cudaStream_t st);
+void ncg_mask_scale_launch(double *z, const uint8_t *mask, double scale, size_t n, cudaStream_t st);
+void ncg_butterworth_launch(double2 *spec, int nx, int ny, double dx, double dy, double kc2, double order,
+                            cudaStream_t st);
+// the launchers below return the number of block partials written
+int ncg_dot2_launch(const double *a, const double *b, const double *c, size_t n, double *part, cudaStream_t st);
+int ncg_dot_launch(const double *a, const double *b, size_t n, double *part, cudaStream_t st);
+int ncg_direction_launch(const double *z, const double *g, double beta, double *d, size_t n, double *part,
+                         cudaStream_t st);
+int ncg_project_launch(double *c, const double *d, double step, double max_update, double c_min, double c_max,
+                       const uint8_t *mask, size_t n, double *part, cudaStream_t st);
+
 // ---- nsfactor.cu (Newton-Schulz Schur inverses, TF32 tensor cores) ---------
 struct NsGeom {
     int n, mt, ntn, kc, ks, per;   // ks == 0: the grid does not fit; Gauss-Jordan only
