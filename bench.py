@@ -206,6 +206,79 @@ def generate_observations(p, solver_cls, torch):
     return Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, [FREQ], Y, mask)
 
 
+def run_dtft(args, torch):
+    """The DTFT of the RF preparation (wust_dtft): 2048-sample float32 RF of
+    256 x 256 transmitter/receiver pairs at 16 frequencies, RF resident in
+    HBM (value) and copied from pinned host memory with Y read back (e2e);
+    the oracle's FP64 NumPy DTFT on 8 transmitters as the CPU baseline."""
+    from waveforminversionust_b200._lib import check, load
+    n_time, n_rx, n_tx, n_f = 2048, 256, 256, 16
+    t = np.arange(n_time) * 5e-8
+    f = np.linspace(3e5, 1.8e6, n_f)
+    rng = np.random.default_rng(0)
+    host = torch.as_tensor(rng.standard_normal((n_tx, n_rx, n_time), dtype=np.float32)).pin_memory()
+    rf = host.cuda()                                   # memory [time, rx, tx], time fastest
+    act = torch.ones((n_rx, n_tx), dtype=torch.uint8, device="cuda")
+    Y = torch.empty((n_f, n_rx, n_tx), dtype=torch.complex64, device="cuda")
+    Yh = torch.empty_like(Y, device="cpu").pin_memory()
+    lib = load()
+    st = torch.cuda.current_stream()
+    tp, fp = t.ctypes.data_as(C.c_void_p), f.ctypes.data_as(C.c_void_p)
+
+    def call(src):
+        check(lib.wust_dtft(tp, n_time, fp, n_f, C.c_void_p(src.data_ptr()), 0, n_rx, n_tx, C.c_void_p(act.data_ptr()),
+                            C.c_void_p(Y.data_ptr()), C.c_void_p(st.cuda_stream)))
+
+    for _ in range(args.warmup):
+        call(rf)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(args.steps):
+        call(rf)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    stage = torch.empty_like(rf)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(args.steps):
+        stage.copy_(host, non_blocking=True)
+        call(stage)
+        Yh.copy_(Y, non_blocking=True)
+    ev1.record()
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1) / args.steps
+    from oracle import prepare_fp64 as o
+    sample = 8
+    p_np = host[:sample].numpy().transpose(2, 1, 0)
+    t0 = time.perf_counter()
+    o.dtft(t, f, p_np, np.ones((sample, n_rx), bool))
+    cpu_s = (time.perf_counter() - t0) * n_tx / sample
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    rf_bytes = n_time * n_rx * n_tx * 4
+    achieved = (rf_bytes + n_f * n_rx * n_tx * 8) / (ms * 1e-3) / 1e9
+    print(json.dumps(dict(
+        metric="rf_preparations_per_second", value=1e3 / ms, unit="preparations/s", n_gpus=1, steps=args.steps,
+        warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+        data="synthetic",
+        config=dict(workload=f"RF DTFT: {n_time} float32 samples x {n_rx} RX x {n_tx} TX, {n_f} frequencies",
+                    l2="RF 512 MB, larger than L2"),
+        e2e=dict(value=1e3 / e2e_ms, unit="preparations/s", h2d_bytes_per_step=rf_bytes,
+                 d2h_bytes_per_step=n_f * n_rx * n_tx * 8),
+        roofline=dict(kernel="dtft_kernel (FP64 CUDA-core GEMM, RF streamed once)", bound="hbm", achieved=achieved,
+                      peak=hbm, unit="GB/s", frac=achieved / hbm,
+                      peak_source="MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s", traffic=None),
+        cpu_baseline=dict(value=1.0 / cpu_s, unit="preparations/s", cores=1, kind="port",
+                          sample=f"oracle FP64 NumPy DTFT of {sample} transmitters, scaled to {n_tx}"))))
+
+
 def run_ncg(args, p, obs, torch):
     """NCG updates of wust_reconstruct (oracle + ROI/filter + direction +
     curvature + step + projection) at the workload's frequency, with the
@@ -281,9 +354,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="c64,c64-refined", help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg"],
+    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft"],
                     help="solve: factor once, then time forward solves of all transmitters (kernel profiling); "
-                         "ncg: time NCG updates of the reconstruction loop, update rules on the device and on the host")
+                         "ncg: time NCG updates of the reconstruction loop, update rules on the device and on the host; "
+                         "dtft: time the RF preparation's DTFT")
     args = ap.parse_args()
     global WORKLOAD, N_TX, FREQ
     WORKLOAD = args.workload
@@ -309,6 +383,9 @@ def main():
     from waveforminversionust_b200.solver import HelmholtzSolver
     lib = _lib.load()
 
+    if args.mode == "dtft":
+        run_dtft(args, torch)
+        return
     p = make_problem(seed=rank)
     ny, nx = p.shape
     if args.mode == "solve":

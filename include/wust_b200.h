@@ -230,6 +230,18 @@ int wust_ncg_project(wust_solver *s, double *c, const double *direction, double 
                      double max_update_mps, double c_min, double c_max, const uint8_t *update_mask,
                      double *relative_update);
 
+/* The DTFT of the RF preparation (wust_prepare.m:30-37):
+ *     Y(tx, rx, k) = single( sum_t exp(-2 pi i f_k t) dt * rf(t, rx, tx) ),
+ * FP64 phases and sums over the record's sample times, the traces of channels
+ * with active(tx, rx) == 0 taken as zero.  time_s (n_time), frequencies_hz
+ * (n_f): host; rf: device [n_time, n_rx, n_tx] column-major, float
+ * (rf_is_double == 0) or double; active: device bytes [n_tx, n_rx]; Y: device
+ * complex single [n_tx, n_rx, n_f].  Rejects nonuniform sampling, frequencies
+ * at or above the saved Nyquist and nonfinite samples on active channels with
+ * the reference's messages.  Synchronizes the stream (NULL: legacy default). */
+int wust_dtft(const double *time_s, int n_time, const double *frequencies_hz, int n_f, const void *rf, int rf_is_double,
+              int n_rx, int n_tx, const uint8_t *active, wust_c64 *Y, void *stream);
+
 /* Counters of the last solve/oracle call: correction solves of the last
  * refined solve, its final relative FP64 residual |b - Hx| / |b| and forward
  * error estimate (refined profiles; -1 otherwise), and the number of kernel

@@ -990,6 +990,45 @@ int wust_ncg_project(wust_solver *s, double *c, const double *direction, double 
     });
 }
 
+int wust_dtft(const double *time_s, int n_time, const double *frequencies_hz, int n_f, const void *rf, int rf_is_double,
+              int n_rx, int n_tx, const uint8_t *active, wust_c64 *Y, void *stream) {
+    return guarded([&] {
+        if (!time_s || !frequencies_hz || !rf || !active || !Y) fail(WUST_ERR_INVALID_INPUT, "dtft arguments missing");
+        if (n_time < 2 || n_f < 1 || n_rx < 1 || n_tx < 1) fail(WUST_ERR_INVALID_INPUT, "Invalid sample times");
+        for (int i = 0; i < n_time; ++i)
+            if (!std::isfinite(time_s[i])) fail(WUST_ERR_INVALID_INPUT, "Invalid sample times");
+        // wust_prepare.m:10-14: uniform sampling, frequencies below the saved Nyquist
+        const double dt = time_s[1] - time_s[0];
+        if (!(dt > 0)) fail(WUST_ERR_INVALID_INPUT, "Nonuniform time");
+        for (int i = 1; i < n_time; ++i)
+            if (std::fabs((time_s[i] - time_s[i - 1]) - dt) > dt * 1e-6) fail(WUST_ERR_INVALID_INPUT, "Nonuniform time");
+        for (int k = 0; k < n_f; ++k)
+            if (!(std::isfinite(frequencies_hz[k]) && frequencies_hz[k] > 0 && frequencies_hz[k] < 0.5 / dt))
+                fail(WUST_ERR_INVALID_INPUT, "Frequency outside saved Nyquist");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        double *t_d = nullptr, *f_d = nullptr;
+        double2 *K = nullptr;
+        int *bad = nullptr;
+        WUST_CUDA(cudaMallocAsync(&t_d, sizeof(double) * n_time, st));
+        WUST_CUDA(cudaMallocAsync(&f_d, sizeof(double) * n_f, st));
+        WUST_CUDA(cudaMallocAsync(&K, sizeof(double2) * (size_t)n_time * n_f, st));
+        WUST_CUDA(cudaMallocAsync(&bad, sizeof(int), st));
+        WUST_CUDA(cudaMemcpyAsync(t_d, time_s, sizeof(double) * n_time, cudaMemcpyHostToDevice, st));
+        WUST_CUDA(cudaMemcpyAsync(f_d, frequencies_hz, sizeof(double) * n_f, cudaMemcpyHostToDevice, st));
+        WUST_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), st));
+        dtft_launch(t_d, f_d, n_time, n_f, dt, rf, rf_is_double != 0, n_rx, n_tx, active, K,
+                    reinterpret_cast<float2 *>(Y), bad, st);
+        int h_bad = 0;
+        WUST_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+        WUST_CUDA(cudaFreeAsync(t_d, st));
+        WUST_CUDA(cudaFreeAsync(f_d, st));
+        WUST_CUDA(cudaFreeAsync(K, st));
+        WUST_CUDA(cudaFreeAsync(bad, st));
+        WUST_CUDA(cudaStreamSynchronize(st));
+        if (h_bad) fail(WUST_ERR_INVALID_INPUT, "Nonfinite RF on an active channel");
+    });
+}
+
 int wust_solver_stats(const wust_solver *s, int *refine_iters, double *final_residual, double *error_estimate,
                       long long *kernel_launches) {
     return guarded([&] {

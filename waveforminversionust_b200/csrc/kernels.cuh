@@ -92,6 +92,12 @@ int ncg_direction_launch(const double *z, const double *g, double beta, double *
 int ncg_project_launch(double *c, const double *d, double step, double max_update, double c_min, double c_max,
                        const uint8_t *mask, size_t n, double *part, cudaStream_t st);
 
+// ---- prepare.cu (DTFT of the RF preparation) --------------------------------
+// time_s, freq, K (nf x nt): device; rf [nt, n_rx, n_tx] float or double;
+// active [n_tx, n_rx] bytes; Y [n_tx, n_rx, nf]; *bad set on a nonfinite active sample.
+void dtft_launch(const double *time_s, const double *freq, int nt, int nf, double dt, const void *rf, bool rf_double,
+                 int n_rx, int n_tx, const uint8_t *active, double2 *K, float2 *Y, int *bad, cudaStream_t st);
+
 // ---- nsfactor.cu (Newton-Schulz Schur inverses, TF32 tensor cores) ---------
 struct NsGeom {
     int n, mt, ntn, kc, ks, per;   // ks == 0: the grid does not fit; Gauss-Jordan only
