@@ -143,6 +143,7 @@ typedef struct {
     int max_sources;               /* largest RHS batch the object will see (0 -> 256) */
     int factor_method;             /* WUST_FACTOR_*: how the Schur pages are inverted */
     int sweep_method;              /* WUST_SWEEP_*: how the TF32 profile runs its sweeps */
+    int correction_precision;      /* WUST_CORRECTION_*: operands of the refinement's correction sweeps */
 } wust_solver_options;
 
 /* Schur-page inversion (no counterpart in the reference, which always uses
@@ -157,6 +158,14 @@ enum wust_factor_method { WUST_FACTOR_DEFAULT = 0, WUST_FACTOR_GAUSS_JORDAN = 1 
  * (formed once per factorization); SEQUENTIAL: one column step after the
  * other on all SMs.  Both apply the same block-LU operator. */
 enum wust_sweep_method { WUST_SWEEP_DEFAULT = 0, WUST_SWEEP_SEQUENTIAL = 1 };
+
+/* Operands of the correction sweeps of the refined TF32 profile (no
+ * counterpart in the reference, which does not refine).  DEFAULT: BF16 pages
+ * and propagators for the correction solves of the chunked sweeps (a
+ * correction only has to be accurate to about 1e-2 for the refinement to
+ * reach its target in the same number of steps; the BF16 operand stream is
+ * half the bytes); SAME: the profile's TF32 operands for every solve. */
+enum wust_correction_precision { WUST_CORRECTION_DEFAULT = 0, WUST_CORRECTION_SAME = 1 };
 
 /* Assemble the nine-point PML operator on the GPU and factorize it.
  * vel, atten: ny x nx (atten may be NULL = zero).  stream may be NULL. */

@@ -180,7 +180,8 @@ def test_chunked_sweeps_match_sequential(ny, nx, S, pml_cells):
     for method in ("default", "sequential"):
         s = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, pml_cells * dx,
                             dict(backend="gpu", stencil_bounds=(1400, 1700)), precision="tf32-refined",
-                            refine_tol=1e-9, max_sources=S, sweep_method=method)
+                            refine_tol=1e-9, max_sources=S, sweep_method=method,
+                            correction_precision="same")
         for adjoint in (False, True):
             r = np.zeros((ny, nx, S), np.complex64)
             g = np.random.default_rng(5 + adjoint)
@@ -195,6 +196,36 @@ def test_chunked_sweeps_match_sequential(ny, nx, S, pml_cells):
         b = sols["sequential", adjoint][1:-1, 1:-1]
         assert rel(a, b) < 1e-7, adjoint
         assert iters["default", adjoint] <= iters["sequential", adjoint] + 1, iters
+
+
+def test_bf16_correction_sweeps_match_tf32_corrections():
+    """The TF32 profile's correction solves on BF16 operands (pages and chunk
+    propagators) reach the same fields as TF32 corrections once refined to
+    1e-9, and at the default 1e-5 target need at most one more correction."""
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    ny, nx, S = 300, 340, 200
+    dx = 0.3e-3
+    x = (np.arange(nx) - (nx - 1) / 2) * dx
+    y = (np.arange(ny) - (ny - 1) / 2) * dx
+    X, Y = np.meshgrid(x, y)
+    c = 1500 + 40 * np.exp(-((X - 2e-3) ** 2 + Y ** 2) / (2 * (8e-3) ** 2))
+    g = np.random.default_rng(9)
+    r = np.zeros((ny, nx, S), np.complex64)
+    r[1:-1, 1:-1] = g.standard_normal((ny - 2, nx - 2, S)) + 1j * g.standard_normal((ny - 2, nx - 2, S))
+    sols, iters = {}, {}
+    for corr in ("default", "same"):
+        for tol in (1e-9, 1e-5):
+            s = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, 16 * dx, dict(backend="gpu", stencil_bounds=(1400, 1700)),
+                                precision="tf32-refined", refine_tol=tol, max_sources=S, correction_precision=corr)
+            for adjoint in (False, True):
+                sols[corr, tol, adjoint] = to_np(s.solve(r, adjoint=adjoint))
+                st = s.stats()
+                assert st["error_estimate"] <= tol, (corr, tol, adjoint, st)
+                iters[corr, tol, adjoint] = st["refine_iters"]
+            s.close()
+    for adjoint in (False, True):
+        assert rel(sols["default", 1e-9, adjoint][1:-1, 1:-1], sols["same", 1e-9, adjoint][1:-1, 1:-1]) < 1e-7
+        assert iters["default", 1e-5, adjoint] <= iters["same", 1e-5, adjoint] + 1, iters
 
 
 def test_newton_schulz_factor_agrees_with_gauss_jordan():

@@ -54,7 +54,7 @@ class SolverOptions(C.Structure):
         ("stencil_vmin", C.c_double), ("stencil_vmax", C.c_double),
         ("dispersion", C.c_int), ("time_step_s", C.c_double), ("reference_speed_mps", C.c_double),
         ("precision", C.c_int), ("refine_max_iters", C.c_int), ("refine_tol", C.c_double),
-        ("max_sources", C.c_int), ("factor_method", C.c_int), ("sweep_method", C.c_int),
+        ("max_sources", C.c_int), ("factor_method", C.c_int), ("sweep_method", C.c_int), ("correction_precision", C.c_int),
     ]
 
 

@@ -157,7 +157,13 @@ struct wust_solver {
     float *ck_z = nullptr, *ck_sb = nullptr;
     float2 *ck_edges = nullptr;
     unsigned *ck_sync = nullptr;
-    TcChunkBuffers chunk_buffers() const { return TcChunkBuffers{ck_lpack, ck_b, ck_z, ck_sb, ck_edges, ck_sync, tc_err}; }
+    // BF16 operands of the correction sweeps (TF32 profile, chunked sweeps)
+    int correction_precision = WUST_CORRECTION_DEFAULT;
+    bool bf16_corrections = false;
+    uint8_t *tc_afwd16 = nullptr, *tc_aadj16 = nullptr, *ck_lpack16 = nullptr;
+    TcChunkBuffers chunk_buffers() const {
+        return TcChunkBuffers{ck_lpack, ck_b, ck_lpack16, ck_z, ck_sb, ck_edges, ck_sync, tc_err};
+    }
     // Newton-Schulz factorization (TF32 profile)
     void *ns_scratch = nullptr;
     NsGeom ns_g{};
@@ -208,7 +214,8 @@ static void free_solver(wust_solver *s) {
                     s->tmp, s->work, s->x64, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
                     s->rx_at, s->Yd, s->maskd, s->resid, s->scale, s->loss_src, s->grad, s->dir, s->ret_u,
                     s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err, s->ns_scratch,
-                    s->ck_lpack, s->ck_b, s->ck_z, s->ck_sb, s->ck_edges, s->ck_sync};
+                    s->ck_lpack, s->ck_b, s->ck_z, s->ck_sb, s->ck_edges, s->ck_sync,
+                    s->tc_afwd16, s->tc_aadj16, s->ck_lpack16};
     for (void *p : ptrs) dfree(p);
     if (s->fft_ready) {
         cufftDestroy(s->fft_fwd);
@@ -293,6 +300,7 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
     }
     if (s->precision == WUST_PRECISION_TF32_REFINED) {
         tc_pack_invT(s->invT, s->ny, s->nx, s->tc_geom, s->tc_afwd, s->tc_aadj, st);
+        if (s->bf16_corrections) tc_pack_invT16(s->invT, s->ny, s->nx, s->ck_geom, s->tc_afwd16, s->tc_aadj16, st);
         if (s->use_chunks) tc_chunk_prepare(s->coefs64(), s->tc_afwd, s->tc_aadj, s->ck_geom, s->chunk_buffers(), st);
     }
     WUST_CUDA(cudaEventRecord(s->ev[2], st));
@@ -335,12 +343,13 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
 
 // One sweep pair (forward+backward) with the profile's arithmetic: CUDA-core
 // complex single, or tcgen05 TF32 GEMMs on the packed invT operands.
-static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
+static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out, bool correction = false) {
     WUST_CUDA(cudaEventRecord(s->sw_ev[0], s->st));
     if (s->precision == WUST_PRECISION_TF32_REFINED) {
+        const bool bf16 = correction && s->bf16_corrections;
         if (s->use_chunks)
-            tc_chunk_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->ck_geom, s->chunk_buffers(), src, S, adjoint,
-                           out, s->st);
+            tc_chunk_solve(s->coefs64(), bf16 ? s->tc_afwd16 : s->tc_afwd, bf16 ? s->tc_aadj16 : s->tc_aadj, s->ck_geom,
+                           s->chunk_buffers(), src, S, adjoint, out, bf16, s->st);
         else
             tc_sweep_solve(s->coefs64(), s->tc_afwd, s->tc_aadj, s->tc_geom, src, S, adjoint, out, s->tc_b,
                            s->tc_part, s->tc_sync, s->tc_err, s->st);
@@ -400,7 +409,7 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
             fail(WUST_ERR_NOT_CONVERGED, "refinement did not reach %.1e after %d correction solves (estimate %.3e)",
                  s->refine_tol, s->refine_max, s->last_error_est);
         rn_prev = rn;
-        run_sweep(s, dense, S, adjoint, s->d32);
+        run_sweep(s, dense, S, adjoint, s->d32, true);
         accumulate_launch(s->d32, s->x64, s->ny, s->nx, S, s->dnorm2, s->xnorm2, st);
         residual_launch(s->coefs128(), src, s->x64, S, adjoint, s->r32, s->rnorm2, nullptr, st);
         WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -562,6 +571,9 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         if (o->sweep_method < WUST_SWEEP_DEFAULT || o->sweep_method > WUST_SWEEP_SEQUENTIAL)
             fail(WUST_ERR_INVALID_INPUT, "unknown sweep_method %d", o->sweep_method);
         s->sweep_method = o->sweep_method;
+        if (o->correction_precision < WUST_CORRECTION_DEFAULT || o->correction_precision > WUST_CORRECTION_SAME)
+            fail(WUST_ERR_INVALID_INPUT, "unknown correction_precision %d", o->correction_precision);
+        s->correction_precision = o->correction_precision;
         s->precision = o->precision;
         s->refine_max = o->refine_max_iters > 0 ? o->refine_max_iters : 8;
         s->refine_tol = o->refine_tol > 0 ? o->refine_tol : 1e-5;
@@ -647,6 +659,12 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
                 WUST_CUDA(cudaMemset(s->ck_sb, 0, s->ck_geom.state_bytes));
                 s->ck_sync = dalloc<unsigned>(s->ck_geom.sync_words);
                 s->ck_edges = dalloc<float2>(s->ck_geom.edge_bytes / sizeof(float2));
+                s->bf16_corrections = s->correction_precision == WUST_CORRECTION_DEFAULT;
+                if (s->bf16_corrections) {
+                    s->tc_afwd16 = dalloc<uint8_t>(s->ck_geom.page_bytes16 * nx);
+                    s->tc_aadj16 = dalloc<uint8_t>(s->ck_geom.page_bytes16 * nx);
+                    if (s->ck_geom.lpack16_bytes) s->ck_lpack16 = dalloc<uint8_t>(s->ck_geom.lpack16_bytes);
+                }
             }
         }
         assemble_and_factor(s, vel, atten);

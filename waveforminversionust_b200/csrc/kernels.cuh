@@ -53,9 +53,12 @@ void tc_sweep_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t 
 // ---- tcchunk.cu (column-chunked tensor-core sweeps, TF32 inputs) -----------
 struct TcChunkGeom {
     int n, mt, kc;        // interior size, 64-row M tiles, 16-row K chunks (same packing as TcSweepGeom)
+    int kc16;             // 32-row K chunks of the BF16 operands
     int C;                // column chunks per substitution
     size_t page_bytes;    // packed operand bytes per page
+    size_t page_bytes16;  // BF16 packed operand bytes per page
     size_t lpack_bytes;   // packed -Lambda_c pages: 4 substitutions x C pages
+    size_t lpack16_bytes; // the same, BF16
     size_t b_bytes;       // packed B chunks of C groups
     size_t state_bytes;   // C column states (re, im planes of 256 sources x ny rows)
     size_t edge_bytes;    // first and last state row of every CTA of C groups
@@ -63,6 +66,7 @@ struct TcChunkGeom {
 };
 struct TcChunkBuffers {
     uint8_t *lpack, *bglob;
+    uint8_t *lpack16;     // nullable: BF16 propagator pages
     float *zst, *sb;      // zero-initialised once (border rows are never written)
     float2 *edges;
     unsigned *sync;
@@ -74,9 +78,14 @@ size_t tc_chunk_state_floats(int ny);
 // Composed propagators of the chunks of all four substitutions (after tc_pack_invT).
 void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
                       const TcChunkBuffers &b, cudaStream_t st);
-// Same contract as tc_sweep_solve: u (ny*nx*S) is overwritten.
+// invT pages -> BF16 packed operands of invT_j and invT_j^H (g.page_bytes16 per page)
+void tc_pack_invT16(const float2 *invT, int ny, int nx, const TcChunkGeom &g, uint8_t *afwd16, uint8_t *aadj16,
+                    cudaStream_t st);
+// Same contract as tc_sweep_solve: u (ny*nx*S) is overwritten.  bf16: afwd /
+// aadj are the BF16 pages and the BF16 propagators are used.
 void tc_chunk_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
-                    const TcChunkBuffers &b, const SrcView &src, int S, bool adjoint, float2 *u, cudaStream_t st);
+                    const TcChunkBuffers &b, const SrcView &src, int S, bool adjoint, float2 *u, bool bf16,
+                    cudaStream_t st);
 
 // ---- ncg.cu (NCG update, FP64) -------------------------------------------------
 constexpr int kNcgMaxBlocks = 592;    // partials per reduction (<= 3 values each)

@@ -37,6 +37,20 @@ __host__ __device__ __forceinline__ size_t chunk_off(int row, int ke) {
     return (size_t)(row >> 3) * kRowGroupBytes + (size_t)(ke >> 2) * 128 + (size_t)(row & 7) * 16 + (ke & 3) * 4;
 }
 
+// The same layout for 16-bit operands: 64 K values per 128-byte chunk row,
+// 8 per 16-byte core-matrix row.
+__host__ __device__ __forceinline__ size_t chunk_off16(int row, int ke) {
+    return (size_t)(row >> 3) * kRowGroupBytes + (size_t)(ke >> 3) * 128 + (size_t)(row & 7) * 16 + (ke & 7) * 2;
+}
+
+// fp32 -> bf16 bits, round to nearest even; Inf and NaN keep their class.
+__device__ __forceinline__ uint16_t to_bf16_bits(float x) {
+    uint32_t u = __float_as_uint(x);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)((u >> 16) | ((u & 0xffffu) ? 0x40u : 0u));
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
 // Round to TF32 (10-bit mantissa, nearest, ties away).  The tensor core
 // would otherwise drop the low mantissa bits of fp32 operands (truncation),
 // a bias that accumulates over long products.  Integer form (two ALU ops):

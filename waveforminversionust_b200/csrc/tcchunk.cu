@@ -42,7 +42,8 @@ constexpr int kCkThreads = 512;
 constexpr int kCkWarps = kCkThreads / 32;
 constexpr int kCkStages = 4;
 constexpr int kCkMaxN = 256;                                     // sources per launch (MMA N)
-constexpr int kCkRowsPerChunk = 16;                              // complex rows per K chunk
+constexpr int kCkRowsPerChunk = 16;                              // complex rows per K chunk (TF32)
+constexpr int kCkRowsPerChunk16 = 32;                            // complex rows per K chunk (BF16)
 constexpr int kCkMaxChunks = 148;
 constexpr size_t kCkBSlot = (size_t)kCkMaxN * tc::kChunkBytes;   // 32 KB
 constexpr size_t kCkSmemRing = (size_t)kCkStages * (tc::kAChunk + kCkBSlot);
@@ -72,6 +73,7 @@ TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas) {
     g.n = ny - 2;
     g.mt = ceil_div(g.n, 64);
     g.kc = ceil_div(g.n, kCkRowsPerChunk);
+    g.kc16 = ceil_div(g.n, kCkRowsPerChunk16);
     const int steps = nx - 1;
     if (steps < 1 || g.n < 1) fail(WUST_ERR_INVALID_INPUT, "chunked sweep needs Nx >= 2 and Ny >= 3");
     if (g.mt > max_ctas)
@@ -83,7 +85,9 @@ TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas) {
     C = std::max(1, std::min({C, max_ctas / g.mt, steps / 2, kCkMaxChunks}));
     g.C = C;
     g.page_bytes = (size_t)g.mt * g.kc * tc::kAChunk;
+    g.page_bytes16 = (size_t)g.mt * g.kc16 * tc::kAChunk;
     g.lpack_bytes = C >= 3 ? (size_t)4 * C * g.page_bytes : 0;
+    g.lpack16_bytes = C >= 3 ? (size_t)4 * C * g.page_bytes16 : 0;
     g.b_bytes = (size_t)C * g.kc * kCkBSlot;
     g.state_bytes = (size_t)C * tc_chunk_state_floats(ny) * sizeof(float);
     g.edge_bytes = (size_t)C * g.mt * 2 * kCkMaxN * sizeof(float2);
@@ -135,7 +139,9 @@ struct ChunkParams {
     unsigned long long timeout_ns;
 };
 
-template <bool ADJ>
+// BF: BF16 operands (kind::f16 MMAs, 32 complex rows per K chunk) for the
+// correction solves of the refinement; TF32 otherwise.
+template <bool ADJ, bool BF>
 __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_constant__ ChunkParams p) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *sA = smem;                                          // [stage] 16 KB
@@ -187,8 +193,10 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         return p.apack + (size_t)((ADJ && f) ? j - 1 : j) * p.page_bytes;
     };
     // incoming state value at grid row y (0 .. ny-1; 0 outside), local source s
+    // (0 for the padding sources beyond s_end: the caller's fields hold only
+    // s_end sources)
     auto cval = [&](int in, const float *pl, int y, int s) -> float2 {
-        if (y < 0 || y >= ny) return f2(0.f, 0.f);
+        if (y < 0 || y >= ny || p.s0 + s >= p.s_end) return f2(0.f, 0.f);
         if (in == IN_PLANES) return f2(__ldcg(pl + (size_t)s * ny + y), __ldcg(pl + (size_t)(kCkMaxN + s) * ny + y));
         if (in == IN_UCOL) return __ldcg(p.u + plane * (p.s0 + s) + (size_t)ny * (nx - 1) + y);
         if (in == IN_IDENT) return f2((y >= 1 && y <= n && y - 1 == p.s0 + s) ? 1.f : 0.f, 0.f);
@@ -341,10 +349,20 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                             if (v1) { __stcg(re + y0 + 1, b1.x); __stcg(im + y0 + 1, b1.y); }
                         }
                     }
-                    bq[4 * h4 + q] = make_float4(to_tf32(b0.x), to_tf32(b0.y), to_tf32(b1.x), to_tf32(b1.y));
+                    if (BF) {
+                        // rows yp0, yp0 + 1 of chunk yp0 / 32: four bf16 values (8 bytes)
+                        if (pack && yp0 < kCkRowsPerChunk16 * kc) {
+                            const int Q = yp0 / kCkRowsPerChunk16, ke = 2 * (yp0 % kCkRowsPerChunk16);
+                            const uint32_t lo = (uint32_t)tc::to_bf16_bits(b0.x) | ((uint32_t)tc::to_bf16_bits(b0.y) << 16);
+                            const uint32_t hi = (uint32_t)tc::to_bf16_bits(b1.x) | ((uint32_t)tc::to_bf16_bits(b1.y) << 16);
+                            *reinterpret_cast<uint2 *>(bg + (size_t)Q * bbytes + tc::chunk_off16(s, ke)) = make_uint2(lo, hi);
+                        }
+                    } else {
+                        bq[4 * h4 + q] = make_float4(to_tf32(b0.x), to_tf32(b0.y), to_tf32(b1.x), to_tf32(b1.y));
+                    }
                 }
             }
-            if (pack) {
+            if (pack && !BF) {
                 float4 *reg = reinterpret_cast<float4 *>(cs + (size_t)grp * 8 * 64);   // 256 float4
                 __syncwarp();
 #pragma unroll
@@ -557,7 +575,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
     }
     float *cur = kind == K_BOUND ? nullptr : p.zst + (size_t)chunk * sfl;
     constexpr int kMmaPerChunk = tc::kChunkBytes / 32;
-    const uint32_t idesc = tc::instr_desc<true>(tc::kTileRows, N);
+    const uint32_t idesc = tc::instr_desc<!BF>(tc::kTileRows, N);
 
 #ifdef WUST_CHUNK_PROFILE
     long long prof_t = clock64();
@@ -576,7 +594,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                 tc::fence_after();
 #pragma unroll
                 for (int kk = 0; kk < kMmaPerChunk; ++kk)
-                    tc::mma<true>(tmem, tc::smem_desc(sA + (size_t)slot * tc::kAChunk + kk * 256),
+                    tc::mma<!BF>(tmem, tc::smem_desc(sA + (size_t)slot * tc::kAChunk + kk * 256),
                                   tc::smem_desc(sB + (size_t)slot * kCkBSlot + kk * 256), idesc,
                                   (q > 0 || kk > 0) ? 1u : 0u);
                 tc::commit(&empty[slot]);
@@ -671,9 +689,12 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
 // -Lambda_c (columns [s0, s_end) of the propagators of chunks 1 .. C-2, in
 // the state planes) -> packed [Ar -Ai; Ai Ar] A pages of the boundary steps
 // (page c), and the rows [s0, s_end) of -Lambda_c^H -> the pages C-1-c of the
-// H^H boundary steps.
+// H^H boundary steps.  BF: BF16 pages (32 complex columns per K chunk).
+template <bool BF>
 __global__ void pack_lambda_kernel(const float *zst, size_t sfl, int ny, int n, int mt, int kc, size_t page_bytes,
                                    int s0, int s_end, int C, uint8_t *lpack, uint8_t *lpack_h) {
+    constexpr int RPC = BF ? kCkRowsPerChunk16 : kCkRowsPerChunk;   // complex columns per chunk
+    constexpr int CPU = RPC / 8;                                      // complex columns per 16-byte unit
     const int i_s = threadIdx.x;                     // stacked row 0..127
     const int Q = blockIdx.x;                        // K chunk
     const int m = blockIdx.y;                        // M tile
@@ -681,50 +702,101 @@ __global__ void pack_lambda_kernel(const float *zst, size_t sfl, int ny, int n, 
     const int i = m * 64 + (i_s & 63);
     const bool imrow = i_s >= 64;
     const float *pl = zst + (size_t)c * sfl;
+    auto store = [&](uint8_t *dst, int u, const float (&v)[2 * CPU]) {
+        if (BF) {
+            uint32_t w[CPU];
+#pragma unroll
+            for (int h = 0; h < CPU; ++h)
+                w[h] = (uint32_t)tc::to_bf16_bits(v[2 * h]) | ((uint32_t)tc::to_bf16_bits(v[2 * h + 1]) << 16);
+            *reinterpret_cast<uint4 *>(dst + tc::chunk_off16(i_s, 8 * u)) = make_uint4(w[0], w[1], w[2 % CPU], w[3 % CPU]);
+        } else {
+            *reinterpret_cast<float4 *>(dst + chunk_off(i_s, 4 * u)) =
+                make_float4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2 % (2 * CPU)]), to_tf32(v[3 % (2 * CPU)]));
+        }
+    };
     // direct: A(i, k) = -Lambda(i, k) for K columns k in [s0, s_end)
-    if ((Q * kCkRowsPerChunk < s_end || s_end >= n) && (Q + 1) * kCkRowsPerChunk > s0) {
+    if ((Q * RPC < s_end || s_end >= n) && (Q + 1) * RPC > s0) {
         uint8_t *dst = lpack + (size_t)c * page_bytes + ((size_t)m * kc + Q) * tc::kAChunk;
 #pragma unroll 2
-        for (int k4 = 0; k4 < 8; ++k4) {
-            float v[4];
+        for (int u = 0; u < 8; ++u) {
+            const int kk = Q * RPC + CPU * u;          // K columns kk .. kk+CPU-1 (the last tile also zeroes the padding)
+            if (!(kk + CPU - 1 >= s0 && (kk < s_end || s_end >= n))) continue;
+            float v[2 * CPU];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int k = Q * kCkRowsPerChunk + 2 * k4 + h;
+            for (int h = 0; h < CPU; ++h) {
+                const int k = kk + h;
                 float2 a = make_float2(0.f, 0.f);
                 if (i < n && k >= s0 && k < s_end) {
-                    const int s = k - s0;
-                    a = make_float2(-pl[(size_t)s * ny + i + 1], -pl[(size_t)(kCkMaxN + s) * ny + i + 1]);
+                    const int sc = k - s0;
+                    a = make_float2(-pl[(size_t)sc * ny + i + 1], -pl[(size_t)(kCkMaxN + sc) * ny + i + 1]);
                 }
                 v[2 * h] = imrow ? a.y : a.x;
                 v[2 * h + 1] = imrow ? a.x : -a.y;
             }
-            const int kk = Q * kCkRowsPerChunk + 2 * k4;   // K columns kk, kk+1 (the last tile also zeroes the padding)
-            if (kk + 1 >= s0 && (kk < s_end || s_end >= n))
-                *reinterpret_cast<float4 *>(dst + chunk_off(i_s, 4 * k4)) =
-                    make_float4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2]), to_tf32(v[3]));
+            store(dst, u, v);
         }
     }
     // conjugate transpose: A(i, k) = -conj(Lambda(k, i)) for rows i in [s0, s_end)
     if (m * 64 >= s0 && m * 64 < s_end) {
         uint8_t *dst = lpack_h + (size_t)(C - 1 - c) * page_bytes + ((size_t)m * kc + Q) * tc::kAChunk;
 #pragma unroll 2
-        for (int k4 = 0; k4 < 8; ++k4) {
-            float v[4];
+        for (int u = 0; u < 8; ++u) {
+            float v[2 * CPU];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int k = Q * kCkRowsPerChunk + 2 * k4 + h;
+            for (int h = 0; h < CPU; ++h) {
+                const int k = Q * RPC + CPU * u + h;
                 float2 a = make_float2(0.f, 0.f);
                 if (i < n && i < s_end && k < n) {
-                    const int s = i - s0;
-                    a = make_float2(-pl[(size_t)s * ny + k + 1], pl[(size_t)(kCkMaxN + s) * ny + k + 1]);
+                    const int sc = i - s0;
+                    a = make_float2(-pl[(size_t)sc * ny + k + 1], pl[(size_t)(kCkMaxN + sc) * ny + k + 1]);
                 }
                 v[2 * h] = imrow ? a.y : a.x;
                 v[2 * h + 1] = imrow ? a.x : -a.y;
             }
-            *reinterpret_cast<float4 *>(dst + chunk_off(i_s, 4 * k4)) =
-                make_float4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2]), to_tf32(v[3]));
+            store(dst, u, v);
         }
     }
+}
+
+// invT pages -> BF16 packed [Ar -Ai; Ai Ar] operands of invT_j and invT_j^H
+// (32 complex columns per K chunk).  One thread per (row of the 128-row tile,
+// chunk, M tile, page).
+__global__ void pack_invT16_kernel(const float2 *__restrict__ invT, int ny, int n, int mt, int kc, size_t page_bytes,
+                                   uint8_t *afwd, uint8_t *aadj) {
+    const int i_s = threadIdx.x;
+    const int c = blockIdx.x, m = blockIdx.y, j = blockIdx.z;
+    const int i = m * 64 + (i_s & 63);
+    const bool imrow = i_s >= 64;
+    const size_t off = (size_t)j * page_bytes + ((size_t)m * kc + c) * tc::kAChunk;
+    const float2 *page = invT + (size_t)j * ny * ny;
+#pragma unroll 2
+    for (int u = 0; u < 8; ++u) {
+        uint32_t wf[4], wa[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int k = c * kCkRowsPerChunk16 + 4 * u + h;
+            float2 af = make_float2(0.f, 0.f), aa = af;
+            if (i < n && k < n) {
+                af = page[(size_t)(i + 1) + (size_t)ny * (k + 1)];
+                const float2 at = page[(size_t)(k + 1) + (size_t)ny * (i + 1)];
+                aa = make_float2(at.x, -at.y);
+            }
+            const float f0 = imrow ? af.y : af.x, f1 = imrow ? af.x : -af.y;
+            const float a0 = imrow ? aa.y : aa.x, a1 = imrow ? aa.x : -aa.y;
+            wf[h] = (uint32_t)tc::to_bf16_bits(f0) | ((uint32_t)tc::to_bf16_bits(f1) << 16);
+            wa[h] = (uint32_t)tc::to_bf16_bits(a0) | ((uint32_t)tc::to_bf16_bits(a1) << 16);
+        }
+        *reinterpret_cast<uint4 *>(afwd + off + tc::chunk_off16(i_s, 8 * u)) = make_uint4(wf[0], wf[1], wf[2], wf[3]);
+        *reinterpret_cast<uint4 *>(aadj + off + tc::chunk_off16(i_s, 8 * u)) = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+    }
+}
+
+void tc_pack_invT16(const float2 *invT, int ny, int nx, const TcChunkGeom &g, uint8_t *afwd16, uint8_t *aadj16,
+                    cudaStream_t st) {
+    const dim3 grid(g.kc16, g.mt, nx);
+    pack_invT16_kernel<<<grid, 128, 0, st>>>(invT, ny, g.n, g.mt, g.kc16, g.page_bytes16, afwd16, aadj16);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
 }
 
 static void ck_configure() {
@@ -732,8 +804,10 @@ static void ck_configure() {
     int dev = 0;
     WUST_CUDA(cudaGetDevice(&dev));
     if (configured_device == dev) return;
-    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
-    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
+    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
+    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
+    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
+    WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
     configured_device = dev;
 }
 
@@ -742,7 +816,7 @@ int tc_chunk_max_ctas() {
     int dev = 0, sms = 0, per_sm = 0;
     WUST_CUDA(cudaGetDevice(&dev));
     WUST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    WUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc_chunk_kernel<false>, kCkThreads, kCkSmem));
+    WUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc_chunk_kernel<false, false>, kCkThreads, kCkSmem));
     return sms * per_sm;
 }
 
@@ -782,21 +856,20 @@ static void set_bounds(ChunkParams &p, int C, bool adjoint, int half) {
     }
 }
 
-static void ck_launch(ChunkParams &p, bool adjoint, int pass, int groups, cudaStream_t st) {
+static void ck_launch(ChunkParams &p, bool adjoint, bool bf16, int pass, int groups, cudaStream_t st) {
     if (groups <= 0) return;
     p.pass = pass;
     WUST_CUDA(cudaMemsetAsync(p.group_ctr, 0, sizeof(unsigned) * groups, st));
     void *args[] = {&p};
     const dim3 grid(groups * p.mt), block(kCkThreads);
-    if (adjoint)
-        WUST_CUDA(cudaLaunchCooperativeKernel((void *)tc_chunk_kernel<true>, grid, block, args, kCkSmem, st));
-    else
-        WUST_CUDA(cudaLaunchCooperativeKernel((void *)tc_chunk_kernel<false>, grid, block, args, kCkSmem, st));
+    void *fn = adjoint ? (bf16 ? (void *)tc_chunk_kernel<true, true> : (void *)tc_chunk_kernel<true, false>)
+                       : (bf16 ? (void *)tc_chunk_kernel<false, true> : (void *)tc_chunk_kernel<false, false>);
+    WUST_CUDA(cudaLaunchCooperativeKernel(fn, grid, block, args, kCkSmem, st));
     ++g_kernel_launches;
 }
 
-static uint8_t *lpack_of(const TcChunkGeom &g, uint8_t *lpack, bool adjoint, int half) {
-    return lpack + (size_t)((adjoint ? 2 : 0) + half) * g.C * g.page_bytes;
+static uint8_t *lpack_of(const TcChunkGeom &g, uint8_t *lpack, bool adjoint, int half, size_t page_bytes) {
+    return lpack + (size_t)((adjoint ? 2 : 0) + half) * g.C * page_bytes;
 }
 
 void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
@@ -813,29 +886,41 @@ void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_
     for (int half = 0; half < 2; ++half) {
         p.half = half;
         set_bounds(p, g.C, false, half);
-        uint8_t *lp = lpack_of(g, b.lpack, false, half);
-        uint8_t *lph = lpack_of(g, b.lpack, true, 1 - half);
+        uint8_t *lp = lpack_of(g, b.lpack, false, half, g.page_bytes);
+        uint8_t *lph = lpack_of(g, b.lpack, true, 1 - half, g.page_bytes);
         for (int s0 = 0; s0 < g.n; s0 += N) {
             p.s0 = s0;
             p.s_end = std::min(g.n, s0 + N);
             p.N = N;
-            ck_launch(p, false, CK_PROP, g.C - 2, st);
+            ck_launch(p, false, false, CK_PROP, g.C - 2, st);
             const dim3 grid(g.kc, g.mt, g.C - 2);
-            pack_lambda_kernel<<<grid, 128, 0, st>>>(b.zst, sfl, co.ny, g.n, g.mt, g.kc, g.page_bytes, s0, p.s_end, g.C,
-                                                     lp, lph);
+            pack_lambda_kernel<false><<<grid, 128, 0, st>>>(b.zst, sfl, co.ny, g.n, g.mt, g.kc, g.page_bytes, s0,
+                                                            p.s_end, g.C, lp, lph);
             ++g_kernel_launches;
+            if (b.lpack16) {
+                const dim3 grid16(g.kc16, g.mt, g.C - 2);
+                pack_lambda_kernel<true><<<grid16, 128, 0, st>>>(
+                    b.zst, sfl, co.ny, g.n, g.mt, g.kc16, g.page_bytes16, s0, p.s_end, g.C,
+                    lpack_of(g, b.lpack16, false, half, g.page_bytes16), lpack_of(g, b.lpack16, true, 1 - half, g.page_bytes16));
+                ++g_kernel_launches;
+            }
         }
     }
     WUST_LAUNCH_CHECK();
 }
 
 void tc_chunk_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
-                    const TcChunkBuffers &b, const SrcView &src, int S, bool adjoint, float2 *u, cudaStream_t st) {
+                    const TcChunkBuffers &b, const SrcView &src, int S, bool adjoint, float2 *u, bool bf16,
+                    cudaStream_t st) {
     ck_configure();
     const int ny = co.ny, nx = co.nx;
     WUST_CUDA(cudaMemsetAsync(u, 0, sizeof(float2) * (size_t)ny * nx * S, st));
     ChunkParams p = base_params(co, g, b);
     p.apack = adjoint ? aadj : afwd;
+    if (bf16) {
+        p.kc = g.kc16;
+        p.page_bytes = g.page_bytes16;
+    }
     p.src = src;
     p.u = u;
     for (int s0 = 0; s0 < S; s0 += kCkMaxN) {
@@ -845,10 +930,11 @@ void tc_chunk_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t 
         for (int half = 0; half < 2; ++half) {
             p.half = half;
             set_bounds(p, g.C, adjoint, half);
-            p.lpack = lpack_of(g, b.lpack, adjoint, half);
-            ck_launch(p, adjoint, CK_FIRST, g.C, st);
-            if (g.C >= 3) ck_launch(p, adjoint, CK_BOUNDARY, 1, st);
-            if (g.C >= 2) ck_launch(p, adjoint, CK_SECOND, g.C - 1, st);
+            p.lpack = bf16 ? lpack_of(g, b.lpack16, adjoint, half, g.page_bytes16)
+                           : lpack_of(g, b.lpack, adjoint, half, g.page_bytes);
+            ck_launch(p, adjoint, bf16, CK_FIRST, g.C, st);
+            if (g.C >= 3) ck_launch(p, adjoint, bf16, CK_BOUNDARY, 1, st);
+            if (g.C >= 2) ck_launch(p, adjoint, bf16, CK_SECOND, g.C - 1, st);
         }
     }
     WUST_LAUNCH_CHECK();

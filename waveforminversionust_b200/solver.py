@@ -61,7 +61,8 @@ class HelmholtzSolver:
     def __init__(self, x, y, vel, atten, f, signConvention, a0, L_PML, options, *,
                  precision: str = "c64", refine_tol: float = 1e-5, refine_max_iters: int = 8,
                  max_sources: int | None = None, stream: torch.cuda.Stream | None = None,
-                 factor_method: str = "default", sweep_method: str = "default"):
+                 factor_method: str = "default", sweep_method: str = "default",
+                 correction_precision: str = "default"):
         if not isinstance(options, dict) or "backend" not in options or "stencil_bounds" not in options:
             raise WustError(1, "Explicit backend and fixed stencil_bounds are required")
         bounds = options["stencil_bounds"]
@@ -107,6 +108,10 @@ class HelmholtzSolver:
         if sweep_method not in sweeps:
             raise WustError(1, f"sweep_method must be one of {sorted(sweeps)}")
         opts.sweep_method = sweeps[sweep_method]
+        corrections = {"default": 0, "same": 1}
+        if correction_precision not in corrections:
+            raise WustError(1, f"correction_precision must be one of {sorted(corrections)}")
+        opts.correction_precision = corrections[correction_precision]
         opts.max_sources = int(max_sources or 256)
         self._opts = opts
         self.precision = precision
