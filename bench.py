@@ -504,8 +504,8 @@ def main():
     if sweep_ms_step >= head["factor_ms"]:
         flop = fl["apply"]
         achieved = flop / (head["sweep_ms_per_launch"] * 1e-3) / 1e12
-        kname = ("tc_chunk_kernel (column-chunked tcgen05 TF32 block-LU sweep pair, 256 sources: per "
-                 "substitution pass 1 + boundary chain + pass 2 = 3 launches)"
+        kname = ("tc_chunk_kernel (column-chunked tcgen05 block-LU sweep pairs, 256 sources, 3 launches per "
+                 "substitution; mean over the step's pairs: 2 TF32 solves + 4 BF16 correction solves)"
                  if args.precision == "tf32-refined" else "sweep kernels (CUDA-core block-LU sweep pair)")
     else:
         flop = fl["factor"]
@@ -514,10 +514,11 @@ def main():
                  if args.precision == "tf32-refined" else "factor_kernel (Schur recursion + Gauss-Jordan inverses)")
     # DRAM bytes of one sweep pair of the dominant kernel (its six launches),
     # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one
-    # pass) at 552^2 with 256 sources: 12.48 GB read + 1.18 GB written
+    # pass) at 552^2 with 256 sources: TF32 pair 12.48 GB read + 1.19 GB
+    # written, BF16 correction pair 8.27 + 1.16 GB; the step runs 2 + 4
     traffic = None
     if flop == fl["apply"] and args.precision == "tf32-refined" and WORKLOAD == "config2":
-        traffic = 13.66e9
+        traffic = (2 * 13.67e9 + 4 * 9.42e9) / 6
     roofline = dict(kernel=kname, bound="tensor", achieved=achieved, peak=peak_tf, unit="TFLOP/s",
                     frac=achieved / peak_tf, peak_source=peak_src, traffic=traffic,
                     traffic_unit="bytes per launch (ncu)", hbm_gbs_achieved=(
