@@ -122,7 +122,9 @@ struct wust_solver {
     size_t fscratch_bytes = 0;
     // sweeps
     float2 *u = nullptr, *lam = nullptr, *tmp = nullptr, *work = nullptr;
-    double2 *x64 = nullptr;
+    double2 *x64 = nullptr, *x64b = nullptr;   // FP64 refinement iterates (alternating)
+    double2 *x64_last = nullptr;                // the one holding the last refined solution
+    double2 *w9f = nullptr, *w9a = nullptr;     // interleaved FP64 weights of H and H^H for the residuals
     float2 *r32 = nullptr, *d32 = nullptr;
     double *rnorm2 = nullptr, *bnorm2 = nullptr, *dnorm2 = nullptr, *xnorm2 = nullptr;
     // objective
@@ -211,7 +213,7 @@ static const char *kCoefNames[9] = {"Dd", "Dl", "Du", "Ld", "Ll", "Lu", "Ud", "U
 static void free_solver(wust_solver *s) {
     if (!s) return;
     void *ptrs[] = {s->vel, s->atten, s->exi, s->eyi, s->mult, s->status, s->invT, s->fscratch, s->u, s->lam,
-                    s->tmp, s->work, s->x64, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
+                    s->tmp, s->work, s->x64, s->x64b, s->w9f, s->w9a, s->r32, s->d32, s->rnorm2, s->bnorm2, s->dnorm2, s->xnorm2, s->tx_lin, s->rx_lin,
                     s->rx_at, s->Yd, s->maskd, s->resid, s->scale, s->loss_src, s->grad, s->dir, s->ret_u,
                     s->stage_d, s->stage_c, s->tc_afwd, s->tc_aadj, s->tc_b, s->tc_part, s->tc_sync, s->tc_err, s->ns_scratch,
                     s->ck_lpack, s->ck_b, s->ck_z, s->ck_sb, s->ck_edges, s->ck_sync,
@@ -280,6 +282,7 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
     WUST_CUDA(cudaMemsetAsync(s->status, 0, 64 * sizeof(int), st));
     WUST_CUDA(cudaEventRecord(s->ev[0], st));
     assemble_launch(in, s->vel, atten_dev, s->exi, s->eyi, s->c128, s->c64, s->mult, s->status, st);
+    if (s->w9f) refine_weights_launch(s->coefs128(), s->w9f, s->w9a, st);
     WUST_CUDA(cudaEventRecord(s->ev[1], st));
     int hstat[3] = {0, 0, 0};
     auto check_assembly = [&](int astat) {
@@ -379,7 +382,8 @@ static void check_tc_err(wust_solver *s) {
 // differ from the dense source buffer.
 //
 // Refinement: x_0 = solve(b); r_k = b - H x_k in FP64; d_{k+1} = solve(r_k);
-// x_{k+1} = x_k + d_{k+1}.  The stopping rule is on the forward error: the
+// x_{k+1} = x_k + d_{k+1}, with x in FP64 (two buffers, one step's input
+// and output) and each step's c64 copy in out.  The stopping rule is on the forward error: the
 // correction d_k measures the error of x_{k-1}, and the residual ratio
 // rho_k = |r_k| / |r_{k-1}| is the contraction of one step, so
 // |e_k| / |x_k| ~ rho_k |d_k| / |x_k|.  Refinement stops when that estimate is
@@ -392,14 +396,14 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
     s->last_residual = -1;
     s->last_error_est = -1;
     if (s->precision == WUST_PRECISION_C64) return;
-    const size_t plane = s->plane();
-    const size_t n = plane * S;
-    promote_launch(out, s->x64, n, st);
     std::vector<double> rn(S), rn_prev(S), bn(S), dn(S), xn(S);
     SrcView dense{};
     dense.mode = SRC_DENSE;
     dense.dense = s->r32;
-    residual_launch(s->coefs128(), src, s->x64, S, adjoint, s->r32, s->rnorm2, s->bnorm2, st);
+    double2 *xa = s->x64, *xb = s->x64b;
+    s->x64_last = xa;
+    const RefineWeights rw{s->w9f, s->w9a, s->ny, s->nx};
+    refine_first_launch(rw, src, out, S, adjoint, xa, s->r32, s->rnorm2, s->bnorm2, st);
     WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
     WUST_CUDA(cudaMemcpyAsync(bn.data(), s->bnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
     WUST_CUDA(cudaStreamSynchronize(st));
@@ -410,8 +414,10 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
                  s->refine_tol, s->refine_max, s->last_error_est);
         rn_prev = rn;
         run_sweep(s, dense, S, adjoint, s->d32, true);
-        accumulate_launch(s->d32, s->x64, s->ny, s->nx, S, s->dnorm2, s->xnorm2, st);
-        residual_launch(s->coefs128(), src, s->x64, S, adjoint, s->r32, s->rnorm2, nullptr, st);
+        refine_step_launch(rw, src, s->d32, xa, S, adjoint, xb, out, s->r32, s->rnorm2, s->dnorm2,
+                           s->xnorm2, st);
+        std::swap(xa, xb);
+        s->x64_last = xa;
         WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaMemcpyAsync(dn.data(), s->dnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaMemcpyAsync(xn.data(), s->xnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -431,7 +437,6 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
         s->last_error_est = worst_err;
         if (worst_err <= s->refine_tol) break;
     }
-    demote_launch(s->x64, out, n, st);
 }
 
 extern "C" {
@@ -626,6 +631,9 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         s->rx_at = dalloc<int32_t>(N);
         if (s->precision != WUST_PRECISION_C64) {
             s->x64 = dalloc<double2>(F);
+            s->x64b = dalloc<double2>(F);
+            s->w9f = dalloc<double2>(9 * N);
+            s->w9a = dalloc<double2>(9 * N);
             s->r32 = dalloc<float2>(F);
             s->d32 = dalloc<float2>(F);
             s->rnorm2 = dalloc<double>(s->smax);
@@ -827,7 +835,7 @@ int wust_solver_oracle(wust_solver *s, const int32_t *tx_index, int n_tx, const 
             fwd.lin = s->tx_lin + first;
             solve_into(s, fwd, nb, false, uf);
             FitParams fp;
-            fp.u = uf; fp.u64 = s->precision == WUST_PRECISION_C64 ? nullptr : s->x64; fp.rx_lin = s->rx_lin; fp.Y = s->Yd; fp.mask = s->maskd;
+            fp.u = uf; fp.u64 = s->precision == WUST_PRECISION_C64 ? nullptr : s->x64_last; fp.rx_lin = s->rx_lin; fp.Y = s->Yd; fp.mask = s->maskd;
             fp.n_tx = n_tx; fp.n_rx = n_rx; fp.first_tx = first; fp.nb = nb; fp.ny = ny; fp.nx = nx;
             fp.residual = s->resid; fp.scale = s->scale + first; fp.loss_per_src = s->loss_src + first;
             fp.status = s->status;

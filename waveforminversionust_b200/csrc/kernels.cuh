@@ -173,14 +173,21 @@ void virtual_source_launch(const float2 *u, const double2 *mult, float2 *virt, i
                            cudaStream_t st);
 
 // ---- refine.cu -------------------------------------------------------------
-// r = b - H x (or H^H) in FP64 on rows y in [1, ny-2]; r64 -> c64 copy for the
-// correction solve; per-source squared norms of r and of b.
-void residual_launch(const Coefs<double2> &co, const SrcView &b, const double2 *x, int S, bool adjoint,
-                     float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st);
-void promote_launch(const float2 *u, double2 *x, size_t n, cudaStream_t st);          // x = u
-// x += d per source plane; per-source squared norms of d and of the new x
-void accumulate_launch(const float2 *d, double2 *x, int ny, int nx, int S, double *dnorm2, double *xnorm2,
-                       cudaStream_t st);
-void demote_launch(const double2 *x, float2 *u, size_t n, cudaStream_t st);           // u = x
+// Interleaved nine-point weights [x][y][9] of H (w9f) and H^H (w9a), complex128.
+struct RefineWeights {
+    const double2 *w9f, *w9a;
+    int ny, nx;
+};
+void refine_weights_launch(const Coefs<double2> &co, double2 *w9f, double2 *w9a, cudaStream_t st);
+// First refinement step: x = u (FP64), r = b - H x (or H^H) on rows
+// y in [1, ny-2], zero on rows 0 and ny-1, as c64 for the correction solve;
+// per-source squared interior norms of r and (if bnorm2) of b.
+void refine_first_launch(const RefineWeights &w, const SrcView &b, const float2 *u, int S, bool adjoint,
+                         double2 *x, float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st);
+// Later steps: x_new = x_old + d, out = c64(x_new), r = b - H x_new; norms of
+// r, d and x_new.  x_new must differ from x_old.
+void refine_step_launch(const RefineWeights &w, const SrcView &b, const float2 *d, const double2 *x_old, int S,
+                        bool adjoint, double2 *x_new, float2 *out, float2 *r32, double *rnorm2, double *dnorm2,
+                        double *xnorm2, cudaStream_t st);
 
 }  // namespace wust
