@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
             if (fqi[m] < 0) continue;
             const int q = fqi[m] >> 8, i = fqi[m] & 255;
             const int yy = y0 - 1 + i, s = s0 + q;
-            const size_t o = (size_t)sl * kRfSrc * RS + q * RS + i;
+            const int o = (sl * kRfSrc + q) * RS + i;
             if (col_ok && yy < ny && s < S) {
                 const size_t g = (size_t)yy + (size_t)ny * c + plane * s;
                 cp_async8(D + o, p.u + g);
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
 #pragma unroll
         for (int m = 0; m < kFieldIter; ++m) {
             if (fqi[m] < 0) continue;
-            const size_t o = (size_t)sl * kRfSrc * RS + (fqi[m] >> 8) * RS + (fqi[m] & 255);
+            const int o = (sl * kRfSrc + (fqi[m] >> 8)) * RS + (fqi[m] & 255);
             const float2 dv = D[o];
             if (STEP) {
                 const double2 xv = X[o];
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
         const int c = x0 - 1 + k;
         const int sl = k & 1;
         const double2 *wsrc = p.w9 + ((size_t)ny * c + y0) * 9;      // rows y0 .. of column c, contiguous
-        double2 *wdst = Wt + (size_t)sl * 9 * R;
+        double2 *wdst = Wt + sl * 9 * R;
 #pragma unroll
         for (int m = 0; m < kWeightIter; ++m) {
             const int e = tid + kRfThreads * m;
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
             for (int e = tid; e < kRfSrc * R; e += kRfThreads) {
                 const int q = e / R, i = e - q * R;
                 const int yy = y0 + i, s = s0 + q;
-                float2 *dst = Bd + (size_t)sl * kRfSrc * R + e;
+                float2 *dst = Bd + sl * kRfSrc * R + e;
                 if (yy <= ny - 2 && s < S) cp_async8(dst, p.b.dense + (size_t)yy + (size_t)ny * c + plane * s);
                 else *dst = make_float2(0.f, 0.f);
             }
@@ -270,17 +270,19 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
             const int slm = (k - 1) % kRfSlots, sl0 = k % kRfSlots, slp = (k + 1) % kRfSlots, slr = k & 1;
             double2 w[9];
 #pragma unroll
-            for (int t = 0; t < 9; ++t) w[t] = Wt[(size_t)slr * 9 * R + row * 9 + t];
+            for (int t = 0; t < 9; ++t) w[t] = Wt[slr * 9 * R + row * 9 + t];
             const int at = mode == SRC_SCATTER ? At[slr * R + row] : -1;
             const int pt = y + ny * c;
             const bool interior = c >= 1 && c <= nx - 2;
+            // element (y, c) of this thread's first source, then one plane per source
+            const size_t oc = (size_t)y + (size_t)ny * c + plane * (size_t)(s0 + half * kRfHalf);
 #pragma unroll
             for (int j = 0; j < kRfHalf; ++j) {
                 const int q = half * kRfHalf + j, s = s0 + q;
                 if (s >= S) break;
-                const double2 *cm = X + ((size_t)slm * kRfSrc + q) * RS + row + 1;   // row y of column c-1
-                const double2 *c0 = X + ((size_t)sl0 * kRfSrc + q) * RS + row + 1;
-                const double2 *cp = X + ((size_t)slp * kRfSrc + q) * RS + row + 1;
+                const double2 *cm = X + (slm * kRfSrc + q) * RS + row + 1;   // row y of column c-1
+                const double2 *c0 = X + (sl0 * kRfSrc + q) * RS + row + 1;
+                const double2 *cp = X + (slp * kRfSrc + q) * RS + row + 1;
                 // h = sum_t w_t v_t as four independent real sums
                 double hrr = 0.0, hii = 0.0, hri = 0.0, hir = 0.0;
 #pragma unroll
@@ -297,21 +299,21 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
                 if (mode == SRC_POINT) {
                     if (lin[j] == pt) bf.x = 1.f;
                 } else if (mode == SRC_DENSE) {
-                    bf = Bd[((size_t)slr * kRfSrc + q) * R + row];
+                    bf = Bd[(slr * kRfSrc + q) * R + row];
                 } else if (mode == SRC_SCATTER) {
                     if (at >= 0) bf = p.b.vals[at + (size_t)p.b.n_slots * s];
                 }
                 const double2 bv = z_from(bf);
                 const double2 rv = zsub(bv, h);
-                const size_t col = (size_t)ny * c + plane * s;
-                p.r32[(size_t)y + col] = c_from(rv);
+                const size_t o = oc + plane * j;
+                p.r32[o] = c_from(rv);
                 const double2 xv = c0[0];
-                p.x_new[(size_t)y + col] = xv;
-                if (STEP) p.out[(size_t)y + col] = c_from(xv);
+                p.x_new[o] = xv;
+                if (STEP) p.out[o] = c_from(xv);
                 if (interior) {
                     rn[j] += zabs2(rv);
                     if (STEP) {
-                        const float2 dv = D[((size_t)sl0 * kRfSrc + q) * RS + row + 1];
+                        const float2 dv = D[(sl0 * kRfSrc + q) * RS + row + 1];
                         an[j] += (double)dv.x * dv.x + (double)dv.y * dv.y;
                         xn[j] += zabs2(xv);
                     } else {
@@ -322,11 +324,11 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
 #pragma unroll
                 for (int side = 0; side < 2; ++side) {
                     if (y != (side == 0 ? 1 : ny - 2)) continue;
-                    const int yb = side == 0 ? 0 : ny - 1;
-                    const double2 xb = c0[yb - y];
-                    p.r32[(size_t)yb + col] = make_float2(0.f, 0.f);
-                    p.x_new[(size_t)yb + col] = xb;
-                    if (STEP) p.out[(size_t)yb + col] = c_from(xb);
+                    const int dyb = side == 0 ? -1 : 1;          // row 0 or ny-1
+                    const double2 xb = c0[dyb];
+                    p.r32[o + dyb] = make_float2(0.f, 0.f);
+                    p.x_new[o + dyb] = xb;
+                    if (STEP) p.out[o + dyb] = c_from(xb);
                 }
             }
         }
