@@ -269,7 +269,9 @@ int wust_solver_sweep_times(const wust_solver *s, double *total_ms, long long *c
 /* Counters of the last factorization (no counterpart in the reference, which
  * always runs cuSOLVER LU per page): out[0] tensor-core GEMMs and out[1] X
  * updates of the Newton-Schulz pages, out[2] pages inverted by Newton-Schulz,
- * out[3] pages inverted by Gauss-Jordan.  Profiles other than
+ * out[3] pages inverted directly: by Gauss-Jordan, or in closed form for the
+ * Dirichlet columns (unit diagonal, no coupling: the identity page, after a
+ * check of the coefficients).  Profiles other than
  * WUST_PRECISION_TF32_REFINED report {0, 0, 0, Nx}. */
 int wust_solver_factor_stats(const wust_solver *s, long long out[4]);
 

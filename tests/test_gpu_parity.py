@@ -250,6 +250,9 @@ def test_newton_schulz_factor_agrees_with_gauss_jordan():
     assert st["newton_schulz_pages"] + st["gauss_jordan_pages"] == nx, st
     assert st["newton_schulz_pages"] >= nx // 2, st
     assert st["gemms"] >= 2 * st["newton_schulz_pages"] - nx, st
+    # the Dirichlet columns' pages are the identity, written in closed form
+    for j in (0, nx - 1):
+        assert np.array_equal(b[1:-1, 1:-1, j], np.eye(ny - 2)), j
     per_page = np.linalg.norm((b - a).reshape(-1, nx), axis=0) / np.linalg.norm(a.reshape(-1, nx), axis=0)
     assert per_page.max() < 5e-3, (per_page.argmax(), per_page.max())
     assert rel(b, a) < 2e-3

@@ -675,6 +675,37 @@ static int ns_launch(const Coefs<float2> &co, float2 *invT, const NsGeom &g, uin
     return h[2];
 }
 
+// Page j of invT in closed form when T_j is the identity: the Dirichlet
+// columns of the operator, whose rows hold only a unit diagonal
+// (ninePointCoefficients.m:33-34).  T_0 = D_0 has no predecessor; for j > 0,
+// T_j = D_j - L_{j-1} X U_{j-1} = D_j when the coupling L_{j-1} is zero.  The
+// kernel writes the identity page and clears ok[0] if D_j is not the
+// identity (unit diagonal, zero off-diagonals) or L_{j-1} is not zero; the
+// caller then inverts the page by Gauss-Jordan.
+__global__ void identity_page_kernel(Coefs<float2> co, float2 *invT, int j, int *ok) {
+    const int ny = co.ny;
+    const size_t page_sz = (size_t)ny * ny;
+    float2 *P = invT + (size_t)j * page_sz;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = tid; i < page_sz; i += nth) {
+        const int r = (int)(i % ny), c = (int)(i / ny);
+        P[i] = make_float2(r == c && r >= 1 && r <= ny - 2 ? 1.f : 0.f, 0.f);
+    }
+    auto zero = [](float2 v) { return v.x == 0.f && v.y == 0.f; };
+    bool good = true;
+    for (size_t y = tid; y < (size_t)ny; y += nth) {
+        const int yy = (int)y;
+        const float2 d = co.dd(yy, j);
+        if (yy >= 1 && yy <= ny - 2 && !(d.x == 1.f && d.y == 0.f)) good = false;
+        if (yy <= ny - 2 && !(zero(co.dl(yy, j)) && zero(co.du(yy, j)))) good = false;
+        if (j > 0) {
+            if (!zero(co.ld(yy, j - 1))) good = false;
+            if (yy <= ny - 2 && !(zero(co.ll(yy, j - 1)) && zero(co.lu(yy, j - 1)))) good = false;
+        }
+    }
+    if (!good) atomicExch(ok, 0);
+}
+
 void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
                size_t gj_scratch_bytes, cudaStream_t st, long long *stats) {
     const int nx = co.nx;
@@ -686,6 +717,21 @@ void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_
             fail(WUST_ERR_SINGULAR_SCHUR_BLOCK, "Schur block %d is singular (pivot %d)", hstat[0] - 1, hstat[1]);
         if (stats) stats[3] += b - a;
     };
+    // the Dirichlet columns' pages in closed form (Gauss-Jordan if the check fails)
+    int *ok = reinterpret_cast<int *>(static_cast<uint8_t *>(ns_scratch) + g.scratch_bytes - 256) + 8;
+    auto identity = [&](int j) -> bool {
+        const int one = 1;
+        int h = 0;
+        WUST_CUDA(cudaMemcpyAsync(ok, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+        identity_page_kernel<<<(int)std::min<size_t>(((size_t)co.ny * co.ny + 255) / 256, 1184), 256, 0, st>>>(
+            co, invT, j, ok);
+        ++g_kernel_launches;
+        WUST_LAUNCH_CHECK();
+        WUST_CUDA(cudaMemcpyAsync(&h, ok, sizeof(int), cudaMemcpyDeviceToHost, st));
+        WUST_CUDA(cudaStreamSynchronize(st));
+        if (h && stats) stats[3] += 1;
+        return h != 0;
+    };
     // the first pages (Dirichlet column and the PML start) and the last one
     // (Dirichlet column) have no usable predecessor
     const int head = std::min(nx, 3);
@@ -693,7 +739,7 @@ void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_
         gj(0, nx);
         return;
     }
-    gj(0, head);
+    gj(identity(0) ? 1 : 0, head);
     int j = head, fallbacks = 0;
     while (j < nx - 1) {
         if (fallbacks >= 16) {                  // not this operator's regime: finish with Gauss-Jordan
@@ -710,7 +756,7 @@ void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_
             j = bad + 1;
         }
     }
-    gj(nx - 1, nx);
+    if (!identity(nx - 1)) gj(nx - 1, nx);
 }
 
 }  // namespace wust
