@@ -89,7 +89,7 @@ extern "C" int wust_ns_profile_reset() {
 struct NsParams {
     Coefs<float2> co;
     float2 *invT;            // [ny, ny, nx] column-major pages
-    float2 *xf;              // current X, fp32 complex, column-major n x n
+    float2 *xf0, *xf1;       // X, fp32 complex, column-major n x n: an update reads one and writes the other
     uint8_t *aT, *aX;        // A-packed T_j and X: [mt][kc] x 16 KB
     uint8_t *bX, *bR;        // B-packed X and R:   [ntn][kc] x 14 KB
     float *part;             // [tile][ks][128][NTN]
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         for (int idx = gtid; idx < n * n; idx += gthreads) {
             const int r = idx % n, c = idx / n;
             const float2 v = X[(size_t)(r + 1) + (size_t)ny * (c + 1)];
-            p.xf[idx] = v;
+            p.xf0[idx] = v;
             put_x_packed(p, p.aX, p.bX, r, c, v);
         }
         for (size_t idx = gtid; idx < (size_t)(p.j1 - p.j0) * 4 * ny; idx += gthreads) {
@@ -370,97 +370,142 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns);
     }
 
+    // ---- T_jt = D_jt - L_{jt-1} X U_{jt-1} (interior, A layout) of this
+    //      CTA's slice, with X = X_{jt-1}.  fill_window puts X's window (the
+    //      slice's rows and columns, one more on each side) into xw; its
+    //      loads are issued after the coefficient loads, so both are in flight
+    const int wr = nr + 2, wc = NTN + 2;
+    float2 *cw_ = xw + (size_t)(kRows / 3 + 3) * (SP + 2);   // [3][NTN] column coefs ud, uu, ul
+    float2 *rw_ = cw_ + 3 * NTN;                            // [6][rows] row coefs ld, ll, lu, dd, dl, du
+    auto build_T = [&](int jt, auto &&fill_window) {
+        const int jm = jt - 1;
+        // coefficients: items [0, 3 NTN) columns, [3 NTN, 3 NTN + 6 nr) rows
+        float2 cf[2];
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const int q = tid + kNsThreads * m;
+            float2 v2 = make_float2(0.f, 0.f);
+            if (q < 3 * NTN) {
+                const int which = q / NTN, cl = q % NTN, C = gcol0 + cl + 1;
+                if (C <= n) v2 = which == 0 ? p.co.ud(C, jm) : which == 1 ? p.co.uu(C - 1, jm) : p.co.ul(C, jm);
+            } else if (q < 3 * NTN + 6 * nr) {
+                const int rt = q - 3 * NTN, which = rt / nr, rl = rt % nr, R = grow0 + rl + 1;
+                if (R <= n) {
+                    if (which == 0) v2 = p.co.ld(R, jm);
+                    else if (which == 1) v2 = p.co.ll(R - 1, jm);
+                    else if (which == 2) v2 = p.co.lu(R, jm);
+                    else if (which == 3) v2 = p.co.dd(R, jt);
+                    else if (which == 4) v2 = p.co.dl(R, jt);        // element (R+1, R)
+                    else if (R >= 2) v2 = p.co.du(R - 1, jt);        // element (R-1, R)
+                }
+            }
+            cf[m] = v2;
+        }
+        fill_window();
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const int q = tid + kNsThreads * m;
+            if (q < 3 * NTN + 6 * nr) cw_[q] = cf[m];       // rw_ follows cw_ directly
+        }
+        __syncthreads();
+        for (int u = tid; u < nr * NTN; u += kNsThreads) {
+            const int cl = u % NTN, rl = u / NTN;
+            const int r = grow0 + rl, c = gcol0 + cl;
+            float2 v = make_float2(0.f, 0.f);
+            if (r < n && c < n) {
+                // D_jt(R, C): dd on the diagonal, dl(C) below (R = C+1), du(R) above (C = R+1)
+                if (r == c) v = rw_[3 * nr + rl];
+                else if (r == c + 1) v = rw_[4 * nr + (rl - 1 >= 0 ? rl - 1 : 0)];
+                else if (r + 1 == c) v = rw_[5 * nr + (rl + 1 < nr ? rl + 1 : rl)];
+                if (r == c + 1 && rl == 0) v = p.co.dl(c + 1, jt);         // pair leaves the slice
+                if (r + 1 == c && rl + 1 >= nr) v = p.co.du(r + 1, jt);
+                const float2 udc = cw_[cl], uuc = cw_[NTN + cl], ulc = cw_[2 * NTN + cl];
+                float2 right[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {               // rows r-1, r, r+1 (window row rl + d)
+                    const float2 *xr = xw + (rl + d) * (SP + 2) + cl;    // columns c-1, c, c+1
+                    float2 acc = cmul(xr[1], udc);
+                    cfma(acc, xr[0], uuc);
+                    cfma(acc, xr[2], ulc);
+                    right[d] = acc;
+                }
+                float2 lr = cmul(rw_[rl], right[1]);
+                cfma(lr, rw_[nr + rl], right[0]);
+                cfma(lr, rw_[2 * nr + rl], right[2]);
+                v = csub(v, lr);
+            }
+            sx[rl * SP + cl] = v;
+        }
+        __syncthreads();
+        write_a(p.aT);
+    };
+    // window of an X held whole in global memory (all loads of a thread in flight)
+    auto window_from = [&](const float2 *X) {
+        constexpr int kWin = ((kRows / 3 + 4) * (NTN + 2) + kNsThreads - 1) / kNsThreads;
+        float2 v[kWin];
+#pragma unroll
+        for (int m = 0; m < kWin; ++m) {
+            const int u = tid + kNsThreads * m;
+            const int rw = u % wr, cwi = u / wr;
+            const int r = grow0 - 1 + rw, c = gcol0 - 1 + cwi;
+            v[m] = (u < wr * wc && r >= 0 && r < n && c >= 0 && c < n) ? X[(size_t)r + (size_t)n * c]
+                                                                        : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int m = 0; m < kWin; ++m) {
+            const int u = tid + kNsThreads * m;
+            if (u < wr * wc) xw[(u % wr) * (SP + 2) + u / wr] = v[m];
+        }
+    };
+    // window of X_{k+1} = X_k + (X_k R_k) right after an update: the slice is
+    // in sx; each halo value is its owner's sum, formed here the same way
+    // (X_k from Xold plus the split-K partials of the owner's tile, in rank
+    // order), so no barrier is needed before the next Schur complement
+    auto window_after_update = [&](const float2 *Xold) {
+        const int n_halo = 2 * wc + 2 * nr;
+        float2 hv = make_float2(0.f, 0.f);
+        int hrw = 0, hcw = 0;
+        if (tid < n_halo) {
+            const int h = tid;
+            if (h < wc) { hrw = 0; hcw = h; }
+            else if (h < 2 * wc) { hrw = nr + 1; hcw = h - wc; }
+            else if (h < 2 * wc + nr) { hrw = 1 + (h - 2 * wc); hcw = 0; }
+            else { hrw = 1 + (h - 2 * wc - nr); hcw = NTN + 1; }
+            const int r = grow0 - 1 + hrw, c = gcol0 - 1 + hcw;
+            if (r >= 0 && r < n && c >= 0 && c < n) {
+                const float *pt = p.part + (size_t)((r / kRows) + p.mt * (c / NTN)) * KS * 128 * NTN;
+                const int rl = r % kRows, cl = c % NTN;
+                float vx = 0.f, vy = 0.f;
+                for (int q = 0; q < KS; ++q) {
+                    vx += __ldcg(pt + ((size_t)q * 128 + rl) * NTN + cl);
+                    vy += __ldcg(pt + ((size_t)q * 128 + rl + kRows) * NTN + cl);
+                }
+                const float2 xo = Xold[(size_t)r + (size_t)n * c];
+                hv = make_float2(xo.x + vx, xo.y + vy);
+            }
+        }
+        for (int u = tid; u < nr * NTN; u += kNsThreads) {
+            const int rl = u / NTN, cl = u % NTN;
+            const bool in = grow0 + rl < n && gcol0 + cl < n;
+            xw[(rl + 1) * (SP + 2) + cl + 1] = in ? sx[rl * SP + cl] : make_float2(0.f, 0.f);
+        }
+        if (tid < n_halo) xw[hrw * (SP + 2) + hcw] = hv;
+    };
+
     int n_gemms = 0, n_updates = 0, failed = -1, cols_done = 0;
+    int cur = 0;                 // xf0 or xf1 holds the current X
+    bool t_ready = false;        // aT already holds the next page's Schur complement
     for (int j = p.j0; j < p.j1 && ok && failed < 0; ++j) {
-        // ---- T_j = D_j - L_{j-1} X U_{j-1}  (interior, A layout) ------------
+        // ---- T_j (unless the last update of page j-1 formed it already) ---
         NSPROF(0);
-        {
-            // window of X_{j-1} around this CTA's slice and the slice's
-            // coefficients -> shared memory (all loads of a thread in flight)
-            const int jm = j - 1;
-            const int wr = nr + 2, wc = NTN + 2;
-            float2 *cw_ = xw + (size_t)(kRows / 3 + 3) * (SP + 2);   // [3][NTN] column coefs ud, uu, ul
-            float2 *rw_ = cw_ + 3 * NTN;                            // [6][rows] row coefs ld, ll, lu, dd, dl, du
-            {
-                constexpr int kWin = ((kRows / 3 + 4) * (NTN + 2) + kNsThreads - 1) / kNsThreads;
-                float2 v[kWin];
-#pragma unroll
-                for (int m = 0; m < kWin; ++m) {
-                    const int u = tid + kNsThreads * m;
-                    const int rw = u % wr, cwi = u / wr;
-                    const int r = grow0 - 1 + rw, c = gcol0 - 1 + cwi;
-                    v[m] = (u < wr * wc && r >= 0 && r < n && c >= 0 && c < n) ? p.xf[(size_t)r + (size_t)n * c]
-                                                                                : make_float2(0.f, 0.f);
-                }
-                // coefficients: items [0, 3 NTN) columns, [3 NTN, 3 NTN + 6 nr) rows
-                float2 cf[2];
-#pragma unroll
-                for (int m = 0; m < 2; ++m) {
-                    const int q = tid + kNsThreads * m;
-                    float2 v2 = make_float2(0.f, 0.f);
-                    if (q < 3 * NTN) {
-                        const int which = q / NTN, cl = q % NTN, C = gcol0 + cl + 1;
-                        if (C <= n) v2 = which == 0 ? p.co.ud(C, jm) : which == 1 ? p.co.uu(C - 1, jm) : p.co.ul(C, jm);
-                    } else if (q < 3 * NTN + 6 * nr) {
-                        const int rt = q - 3 * NTN, which = rt / nr, rl = rt % nr, R = grow0 + rl + 1;
-                        if (R <= n) {
-                            if (which == 0) v2 = p.co.ld(R, jm);
-                            else if (which == 1) v2 = p.co.ll(R - 1, jm);
-                            else if (which == 2) v2 = p.co.lu(R, jm);
-                            else if (which == 3) v2 = p.co.dd(R, j);
-                            else if (which == 4) v2 = p.co.dl(R, j);        // element (R+1, R)
-                            else if (R >= 2) v2 = p.co.du(R - 1, j);        // element (R-1, R)
-                        }
-                    }
-                    cf[m] = v2;
-                }
-#pragma unroll
-                for (int m = 0; m < kWin; ++m) {
-                    const int u = tid + kNsThreads * m;
-                    if (u < wr * wc) xw[(u % wr) * (SP + 2) + u / wr] = v[m];
-                }
-#pragma unroll
-                for (int m = 0; m < 2; ++m) {
-                    const int q = tid + kNsThreads * m;
-                    if (q < 3 * NTN + 6 * nr) cw_[q] = cf[m];       // rw_ follows cw_ directly
-                }
-            }
-            __syncthreads();
-            for (int u = tid; u < nr * NTN; u += kNsThreads) {
-                const int cl = u % NTN, rl = u / NTN;
-                const int r = grow0 + rl, c = gcol0 + cl;
-                float2 v = make_float2(0.f, 0.f);
-                if (r < n && c < n) {
-                    // D_j(R, C): dd on the diagonal, dl(C) below (R = C+1), du(R) above (C = R+1)
-                    if (r == c) v = rw_[3 * nr + rl];
-                    else if (r == c + 1) v = rw_[4 * nr + (rl - 1 >= 0 ? rl - 1 : 0)];
-                    else if (r + 1 == c) v = rw_[5 * nr + (rl + 1 < nr ? rl + 1 : rl)];
-                    if (r == c + 1 && rl == 0) v = p.co.dl(c + 1, j);         // pair leaves the slice
-                    if (r + 1 == c && rl + 1 >= nr) v = p.co.du(r + 1, j);
-                    const float2 udc = cw_[cl], uuc = cw_[NTN + cl], ulc = cw_[2 * NTN + cl];
-                    float2 right[3];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {               // rows r-1, r, r+1 (window row rl + d)
-                        const float2 *xr = xw + (rl + d) * (SP + 2) + cl;    // columns c-1, c, c+1
-                        float2 acc = cmul(xr[1], udc);
-                        cfma(acc, xr[0], uuc);
-                        cfma(acc, xr[2], ulc);
-                        right[d] = acc;
-                    }
-                    float2 lr = cmul(rw_[rl], right[1]);
-                    cfma(lr, rw_[nr + rl], right[0]);
-                    cfma(lr, rw_[2 * nr + rl], right[2]);
-                    v = csub(v, lr);
-                }
-                sx[rl * SP + cl] = v;
-            }
-            __syncthreads();
-            write_a(p.aT);
+        if (!t_ready) {
+            build_T(j, [&] { window_from(cur ? p.xf1 : p.xf0); });
             NSPROF(5);
             epoch += (unsigned)nblocks;
             if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
             NSPROF(6);
         }
+        t_ready = false;
 
         float r_prev = 0.f;
         bool accepted = false;
@@ -534,14 +579,14 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 break;
             }
             if (dec == 0) {
-                // X_k stays: copy it into page j
+                // X_k stays: copy it into page j.  No barrier: nothing of the
+                // next page's Schur complement writes what another CTA reads
                 float2 *page = p.invT + (size_t)j * page_sz;
-                read_cm(p.xf, (size_t)n);
+                read_cm(cur ? p.xf1 : p.xf0, (size_t)n);
                 __syncthreads();
                 write_cm(page + ny + 1, (size_t)ny);
+                __syncthreads();
                 accepted = true;
-                epoch += (unsigned)nblocks;
-                if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
                 break;
             }
             // ---- X_{k+1} = X_k + X_k R_k ------------------------------------
@@ -551,7 +596,9 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             const bool last = (dec == 1);
             NSPROF(0);
             float2 *page = p.invT + (size_t)j * page_sz;
-            read_cm(p.xf, (size_t)n);                  // X_k of the slice
+            const float2 *xold = cur ? p.xf1 : p.xf0;
+            float2 *xnew = cur ? p.xf0 : p.xf1;
+            read_cm(xold, (size_t)n);                  // X_k of the slice
             float2 pvx[kEpi];
             tile_values(pvx);
             __syncthreads();
@@ -564,10 +611,18 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 x = make_float2(x.x + pvx[m].x, x.y + pvx[m].y);
             }
             __syncthreads();
-            write_cm(p.xf, (size_t)n);
+            write_cm(xnew, (size_t)n);
             if (last) write_cm(page + ny + 1, (size_t)ny);
             write_a(p.aX);
             write_b(p.bX);
+            if (last && j + 1 < p.j1) {
+                // the next page's Schur complement from X_{k+1} (window
+                // formed without a barrier), ready at this update's barrier
+                __syncthreads();
+                build_T(j + 1, [&] { window_after_update(xold); });
+                t_ready = true;
+            }
+            cur ^= 1;
             NSPROF(9);
             epoch += (unsigned)nblocks;
             if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
@@ -606,7 +661,7 @@ NsGeom ns_geom(int ny, int max_ctas) {
     g.a_bytes = (size_t)g.mt * g.kc * tc::kAChunk;
     g.b_bytes = (size_t)g.ntn * g.kc * kBChunkNs;
     g.part_bytes = (size_t)tiles * std::max(g.ks, 1) * 128 * NTN * sizeof(float);
-    g.scratch_bytes = 2 * g.a_bytes + 2 * g.b_bytes + g.part_bytes + (size_t)g.n * g.n * sizeof(float2) +
+    g.scratch_bytes = 2 * g.a_bytes + 2 * g.b_bytes + g.part_bytes + 2 * (size_t)g.n * g.n * sizeof(float2) +
                       (size_t)max_ctas * sizeof(double) + 256;
     return g;
 }
@@ -637,7 +692,8 @@ static int ns_launch(const Coefs<float2> &co, float2 *invT, const NsGeom &g, uin
     p.bX = q; q += g.b_bytes;
     p.bR = q; q += g.b_bytes;
     p.part = reinterpret_cast<float *>(q); q += g.part_bytes;
-    p.xf = reinterpret_cast<float2 *>(q); q += (size_t)g.n * g.n * sizeof(float2);
+    p.xf0 = reinterpret_cast<float2 *>(q); q += (size_t)g.n * g.n * sizeof(float2);
+    p.xf1 = reinterpret_cast<float2 *>(q); q += (size_t)g.n * g.n * sizeof(float2);
     p.rn = reinterpret_cast<double *>(q); q += (size_t)g.mt * g.ntn * g.ks * sizeof(double);
     int *tail = reinterpret_cast<int *>(scratch + g.scratch_bytes - 256);
     p.ctr = reinterpret_cast<unsigned *>(tail);
