@@ -228,6 +228,36 @@ def test_bf16_correction_sweeps_match_tf32_corrections():
         assert iters["default", 1e-5, adjoint] <= iters["same", 1e-5, adjoint] + 1, iters
 
 
+def test_single_correction_returns_the_corrected_field():
+    """With a loose target the refinement stops after one correction; the
+    returned field is then the corrected iterate (the first correction reads
+    the solve's c64 field and writes only the FP64 iterate, whose c64 copy is
+    returned), not the uncorrected solve: its error against a 1e-9 solution is
+    about the estimate, a hundredth of the correction itself."""
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    ny, nx, S = 130, 150, 16
+    dx = 0.3e-3
+    x = (np.arange(nx) - (nx - 1) / 2) * dx
+    y = (np.arange(ny) - (ny - 1) / 2) * dx
+    X, Y = np.meshgrid(x, y)
+    c = 1500 + 40 * np.exp(-((X - 2e-3) ** 2 + Y ** 2) / (2 * (8e-3) ** 2))
+    g = np.random.default_rng(11)
+    r = np.zeros((ny, nx, S), np.complex64)
+    r[1:-1, 1:-1] = g.standard_normal((ny - 2, nx - 2, S)) + 1j * g.standard_normal((ny - 2, nx - 2, S))
+    out = {}
+    for tol in (1e-9, 3e-2):
+        s = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, 16 * dx, dict(backend="gpu", stencil_bounds=(1400, 1700)),
+                            precision="tf32-refined", refine_tol=tol, max_sources=S)
+        for adjoint in (False, True):
+            out[tol, adjoint] = (to_np(s.solve(r, adjoint=adjoint)), s.stats())
+        s.close()
+    for adjoint in (False, True):
+        u1, st = out[3e-2, adjoint]
+        assert st["refine_iters"] == 1, st
+        err = rel(u1[1:-1, 1:-1], out[1e-9, adjoint][0][1:-1, 1:-1])
+        assert err <= 10 * st["error_estimate"] + 1e-6, (adjoint, err, st)
+
+
 def test_newton_schulz_factor_agrees_with_gauss_jordan():
     """The TF32 profile's Schur inverses (Newton-Schulz iterations on the
     tensor cores, Gauss-Jordan on the pages where the previous inverse is no

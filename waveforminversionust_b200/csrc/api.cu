@@ -382,8 +382,9 @@ static void check_tc_err(wust_solver *s) {
 // differ from the dense source buffer.
 //
 // Refinement: x_0 = solve(b); r_k = b - H x_k in FP64; d_{k+1} = solve(r_k);
-// x_{k+1} = x_k + d_{k+1}, with x in FP64 (two buffers, one step's input
-// and output) and each step's c64 copy in out.  The stopping rule is on the forward error: the
+// x_{k+1} = x_k + d_{k+1}, with x_0 the solve's c64 output, later x in FP64
+// (two buffers, one step's input and output) and, from the second
+// correction on, each step's c64 copy in out.  The stopping rule is on the forward error: the
 // correction d_k measures the error of x_{k-1}, and the residual ratio
 // rho_k = |r_k| / |r_{k-1}| is the contraction of one step, so
 // |e_k| / |x_k| ~ rho_k |d_k| / |x_k|.  Refinement stops when that estimate is
@@ -400,10 +401,9 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
     SrcView dense{};
     dense.mode = SRC_DENSE;
     dense.dense = s->r32;
-    double2 *xa = s->x64, *xb = s->x64b;
-    s->x64_last = xa;
+    double2 *xa = nullptr, *xb = s->x64;         // the current FP64 iterate (none yet) and the next one
     const RefineWeights rw{s->w9f, s->w9a, s->ny, s->nx};
-    refine_first_launch(rw, src, out, S, adjoint, xa, s->r32, s->rnorm2, s->bnorm2, st);
+    refine_first_launch(rw, src, out, S, adjoint, s->r32, s->rnorm2, s->bnorm2, st);
     WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
     WUST_CUDA(cudaMemcpyAsync(bn.data(), s->bnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
     WUST_CUDA(cudaStreamSynchronize(st));
@@ -414,9 +414,16 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
                  s->refine_tol, s->refine_max, s->last_error_est);
         rn_prev = rn;
         run_sweep(s, dense, S, adjoint, s->d32, true);
-        refine_step_launch(rw, src, s->d32, xa, S, adjoint, xb, out, s->r32, s->rnorm2, s->dnorm2,
-                           s->xnorm2, st);
-        std::swap(xa, xb);
+        if (!xa) {
+            refine_step_launch(rw, src, s->d32, out, nullptr, S, adjoint, xb, nullptr, s->r32, s->rnorm2, s->dnorm2,
+                               s->xnorm2, st);
+            xa = xb;
+            xb = s->x64b;
+        } else {
+            refine_step_launch(rw, src, s->d32, nullptr, xa, S, adjoint, xb, out, s->r32, s->rnorm2, s->dnorm2,
+                               s->xnorm2, st);
+            std::swap(xa, xb);
+        }
         s->x64_last = xa;
         WUST_CUDA(cudaMemcpyAsync(rn.data(), s->rnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaMemcpyAsync(dn.data(), s->dnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -437,6 +444,7 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
         s->last_error_est = worst_err;
         if (worst_err <= s->refine_tol) break;
     }
+    if (s->last_refine_iters == 1) refine_demote_launch(xa, out, s->plane() * S, st);   // out still holds x_0
 }
 
 extern "C" {

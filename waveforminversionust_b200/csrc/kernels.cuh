@@ -179,15 +179,19 @@ struct RefineWeights {
     int ny, nx;
 };
 void refine_weights_launch(const Coefs<double2> &co, double2 *w9f, double2 *w9a, cudaStream_t st);
-// First refinement step: x = u (FP64), r = b - H x (or H^H) on rows
-// y in [1, ny-2], zero on rows 0 and ny-1, as c64 for the correction solve;
-// per-source squared interior norms of r and (if bnorm2) of b.
+// First refinement step: r = b - H u (or H^H) on rows y in [1, ny-2], zero on
+// rows 0 and ny-1, as c64 for the correction solve; per-source squared
+// interior norms of r and (if bnorm2) of b.
 void refine_first_launch(const RefineWeights &w, const SrcView &b, const float2 *u, int S, bool adjoint,
-                         double2 *x, float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st);
-// Later steps: x_new = x_old + d, out = c64(x_new), r = b - H x_new; norms of
-// r, d and x_new.  x_new must differ from x_old.
-void refine_step_launch(const RefineWeights &w, const SrcView &b, const float2 *d, const double2 *x_old, int S,
-                        bool adjoint, double2 *x_new, float2 *out, float2 *r32, double *rnorm2, double *dnorm2,
-                        double *xnorm2, cudaStream_t st);
+                         float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st);
+// Later steps: x_new = x_old + d in FP64 and r = b - H x_new, with norms of r,
+// d and x_new.  The first correction passes the solve's c64 field as x_old32
+// and no out; later ones pass the FP64 iterate as x_old and get its c64 copy
+// in out.  x_new must differ from x_old.
+void refine_step_launch(const RefineWeights &w, const SrcView &b, const float2 *d, const float2 *x_old32,
+                        const double2 *x_old, int S, bool adjoint, double2 *x_new, float2 *out, float2 *r32,
+                        double *rnorm2, double *dnorm2, double *xnorm2, cudaStream_t st);
+// u = c64(x)
+void refine_demote_launch(const double2 *x, float2 *u, size_t n, cudaStream_t st);
 
 }  // namespace wust

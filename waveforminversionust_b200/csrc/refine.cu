@@ -13,8 +13,10 @@
 //
 // One kernel does each refinement step's elementwise work in one pass over
 // the fields:
-//   first step   x_0 = u (FP64 copy of the solve's c64 field), r_0 = b - H x_0
-//   later steps  x_{k+1} = x_k + d (into the other FP64 buffer), the c64
+//   RF_FIRST     r_0 = b - H u, with x_0 = u the solve's c64 field
+//   RF_STEP_C64  x_1 = u + d in FP64, r_1 = b - H x_1 (u read from the
+//                solve's output, which this step leaves alone)
+//   RF_STEP      x_{k+1} = x_k + d (into the other FP64 buffer), the c64
 //                copy of x_{k+1} into the solve's output, r = b - H x_{k+1}
 // with the per-source squared norms of r, b (first step) and d, x (later
 // steps).  A block owns a tile of up to 94 grid rows, 8 sources and a strip
@@ -45,14 +47,17 @@ constexpr int kRfCols = 48;                        // target strip width
 constexpr int kFieldIter = (kRfSrc * (kRfRows + 2) + kRfThreads - 1) / kRfThreads;   // field entries per thread
 constexpr int kWeightIter = (9 * kRfRows + kRfThreads - 1) / kRfThreads;             // weight entries per thread
 
+enum RefineMode { RF_FIRST = 0, RF_STEP_C64 = 1, RF_STEP = 2 };
+
 struct RefineParams {
     int ny, nx;
     const double2 *w9;      // interleaved weights [x][y][9] of H or H^H
     SrcView b;
     const float2 *u;        // first step: the solve's field; later steps: the correction d
-    const double2 *x_old;   // later steps: x_k
-    double2 *x_new;         // x_0 or x_{k+1}, every grid point
-    float2 *out;            // later steps: c64 copy of x_{k+1}, every grid point
+    const float2 *x_old32;  // RF_STEP_C64: x_0, c64
+    const double2 *x_old;   // RF_STEP: x_k
+    double2 *x_new;         // steps: x_{k+1}, every grid point
+    float2 *out;            // RF_STEP: c64 copy of x_{k+1}, every grid point
     float2 *r32;            // residual, c64, every grid point (zero on rows 0 and ny-1)
     double *rnorm2, *bnorm2, *dnorm2, *xnorm2;
     int S, R, TX;
@@ -142,8 +147,9 @@ __global__ void refine_weights_kernel(Coefs<double2> co, double2 *w9f, double2 *
     }
 }
 
-template <bool ADJ, bool STEP>
+template <bool ADJ, int MODE>
 __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParams p) {
+    constexpr bool STEP = MODE != RF_FIRST;
     extern __shared__ __align__(16) uint8_t rf_smem[];
     const int ny = p.ny, nx = p.nx, S = p.S, R = p.R;
     const int RS = R + 2;                                      // slot rows: the tile and one row above and below
@@ -185,14 +191,15 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
             if (col_ok && yy < ny && s < S) {
                 const size_t g = (size_t)yy + (size_t)ny * c + plane * s;
                 cp_async8(D + o, p.u + g);
-                if (STEP) cp_async16(X + o, p.x_old + g);
+                if (MODE == RF_STEP) cp_async16(X + o, p.x_old + g);
+                if (MODE == RF_STEP_C64) cp_async8(X + o, p.x_old32 + g);   // first half of the slot
             } else {
                 D[o] = make_float2(0.f, 0.f);
                 if (STEP) X[o] = make_double2(0.0, 0.0);
             }
         }
     };
-    // the entries this thread loaded: x = x_old + d, or x = u
+    // the entries this thread loaded: x = x_old + d, or x = u (FP64 sums)
     auto convert = [&](int k) {
         const int sl = k % kRfSlots;
 #pragma unroll
@@ -200,9 +207,12 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
             if (fqi[m] < 0) continue;
             const int o = (sl * kRfSrc + (fqi[m] >> 8)) * RS + (fqi[m] & 255);
             const float2 dv = D[o];
-            if (STEP) {
+            if (MODE == RF_STEP) {
                 const double2 xv = X[o];
                 X[o] = make_double2(xv.x + (double)dv.x, xv.y + (double)dv.y);
+            } else if (MODE == RF_STEP_C64) {
+                const float2 xv = *reinterpret_cast<const float2 *>(X + o);
+                X[o] = make_double2((double)xv.x + (double)dv.x, (double)xv.y + (double)dv.y);
             } else {
                 X[o] = z_from(dv);
             }
@@ -308,8 +318,8 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
                 const size_t o = oc + plane * j;
                 p.r32[o] = c_from(rv);
                 const double2 xv = c0[0];
-                p.x_new[o] = xv;
-                if (STEP) p.out[o] = c_from(xv);
+                if (STEP) p.x_new[o] = xv;
+                if (MODE == RF_STEP) p.out[o] = c_from(xv);
                 if (interior) {
                     rn[j] += zabs2(rv);
                     if (STEP) {
@@ -327,8 +337,8 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
                     const int dyb = side == 0 ? -1 : 1;          // row 0 or ny-1
                     const double2 xb = c0[dyb];
                     p.r32[o + dyb] = make_float2(0.f, 0.f);
-                    p.x_new[o + dyb] = xb;
-                    if (STEP) p.out[o + dyb] = c_from(xb);
+                    if (STEP) p.x_new[o + dyb] = xb;
+                    if (MODE == RF_STEP) p.out[o + dyb] = c_from(xb);
                 }
             }
         }
@@ -356,20 +366,28 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
     }
 }
 
-template <bool ADJ, bool STEP>
+template <bool ADJ, int MODE>
 void refine_launch_one(const RefineParams &p, dim3 grid, size_t smem, cudaStream_t st) {
     static thread_local int configured_device = -1;
     int dev = 0;
     WUST_CUDA(cudaGetDevice(&dev));
     if (configured_device != dev) {
-        WUST_CUDA(cudaFuncSetAttribute(refine_kernel<ADJ, STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        WUST_CUDA(cudaFuncSetAttribute(refine_kernel<ADJ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)refine_smem_bytes(kRfRows)));
         configured_device = dev;
     }
-    refine_kernel<ADJ, STEP><<<grid, kRfThreads, smem, st>>>(p);
+    refine_kernel<ADJ, MODE><<<grid, kRfThreads, smem, st>>>(p);
 }
 
-void refine_launch(RefineParams &p, bool adjoint, bool step, cudaStream_t st) {
+template <bool ADJ>
+void refine_launch_mode(const RefineParams &p, int mode, dim3 grid, size_t smem, cudaStream_t st) {
+    if (mode == RF_FIRST) refine_launch_one<ADJ, RF_FIRST>(p, grid, smem, st);
+    else if (mode == RF_STEP_C64) refine_launch_one<ADJ, RF_STEP_C64>(p, grid, smem, st);
+    else refine_launch_one<ADJ, RF_STEP>(p, grid, smem, st);
+}
+
+void refine_launch(RefineParams &p, bool adjoint, int mode, cudaStream_t st) {
+    const bool step = mode != RF_FIRST;
     const int ny = p.ny, nx = p.nx;
     const int rows = ny - 2;
     const int row_tiles = ceil_div(rows, kRfRows);
@@ -385,13 +403,8 @@ void refine_launch(RefineParams &p, bool adjoint, bool step, cudaStream_t st) {
     } else if (p.bnorm2) {
         WUST_CUDA(cudaMemsetAsync(p.bnorm2, 0, sizeof(double) * p.S, st));
     }
-    if (adjoint) {
-        if (step) refine_launch_one<true, true>(p, grid, smem, st);
-        else refine_launch_one<true, false>(p, grid, smem, st);
-    } else {
-        if (step) refine_launch_one<false, true>(p, grid, smem, st);
-        else refine_launch_one<false, false>(p, grid, smem, st);
-    }
+    if (adjoint) refine_launch_mode<true>(p, mode, grid, smem, st);
+    else refine_launch_mode<false>(p, mode, grid, smem, st);
     ++g_kernel_launches;
     WUST_LAUNCH_CHECK();
 }
@@ -405,26 +418,39 @@ void refine_weights_launch(const Coefs<double2> &co, double2 *w9f, double2 *w9a,
     WUST_LAUNCH_CHECK();
 }
 
+__global__ void demote_kernel(const double2 *x, float2 *u, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        u[i] = c_from(x[i]);
+}
+
+void refine_demote_launch(const double2 *x, float2 *u, size_t n, cudaStream_t st) {
+    demote_kernel<<<(int)std::min<size_t>((n + 255) / 256, 148 * 32), 256, 0, st>>>(x, u, n);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
 void refine_first_launch(const RefineWeights &w, const SrcView &b, const float2 *u, int S, bool adjoint,
-                         double2 *x, float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st) {
+                         float2 *r32, double *rnorm2, double *bnorm2, cudaStream_t st) {
     RefineParams p{};
     p.ny = w.ny;
     p.nx = w.nx;
     p.w9 = adjoint ? w.w9a : w.w9f;
     p.b = b;
     p.u = u;
-    p.x_new = x;
     p.r32 = r32;
     p.rnorm2 = rnorm2;
     p.bnorm2 = bnorm2;
     p.S = S;
-    refine_launch(p, adjoint, false, st);
+    refine_launch(p, adjoint, RF_FIRST, st);
 }
 
-void refine_step_launch(const RefineWeights &w, const SrcView &b, const float2 *d, const double2 *x_old, int S,
-                        bool adjoint, double2 *x_new, float2 *out, float2 *r32, double *rnorm2, double *dnorm2,
-                        double *xnorm2, cudaStream_t st) {
+void refine_step_launch(const RefineWeights &w, const SrcView &b, const float2 *d, const float2 *x_old32,
+                        const double2 *x_old, int S, bool adjoint, double2 *x_new, float2 *out, float2 *r32,
+                        double *rnorm2, double *dnorm2, double *xnorm2, cudaStream_t st) {
+    if ((x_old32 == nullptr) == (x_old == nullptr) || (x_old32 && out) || (x_old && !out))
+        fail(WUST_ERR_RUNTIME, "refinement step: one previous iterate (c64 without output, FP64 with output)");
     RefineParams p{};
+    p.x_old32 = x_old32;
     p.ny = w.ny;
     p.nx = w.nx;
     p.w9 = adjoint ? w.w9a : w.w9f;
@@ -438,7 +464,7 @@ void refine_step_launch(const RefineWeights &w, const SrcView &b, const float2 *
     p.dnorm2 = dnorm2;
     p.xnorm2 = xnorm2;
     p.S = S;
-    refine_launch(p, adjoint, true, st);
+    refine_launch(p, adjoint, x_old32 ? RF_STEP_C64 : RF_STEP, st);
 }
 
 }  // namespace wust
