@@ -128,3 +128,53 @@ def test_tensor_core_profile_edge_cases(small):
         HelmholtzSolver(xg, xg, np.full((n, n), 1500.0), None, 5e5, -1, 10.0, 16 * 3e-4, opts,
                         precision="tf32-refined", max_sources=4)
     assert e.value.identifier == "WUST:InvalidInput"
+
+
+@pytest.mark.parametrize("precision", ["c64-refined", "tf32-refined"])
+def test_reconstruction_final_sound_speed_matches_oracle(precision):
+    """Four NCG updates over two frequencies (wust_reconstruct.m:20-74) on an
+    80 x 80 grid with 8 transmitters and a 32-element ring: the final sound
+    speed of the device loop is within 0.5 m/s RMS of the FP64 oracle's
+    reconstruction (the accuracy bar of the refined solver), asserted with a
+    tenfold margin, after the reconstruction moved the model by more than 1 m/s."""
+    from oracle import helmholtz_fp64 as o
+    from waveforminversionust_b200 import synthetic
+    from waveforminversionust_b200.objective import POOL
+    from waveforminversionust_b200.reconstruct import wust_reconstruct
+    p = synthetic._problem("recon80", 64, 8, 0.5e-3, 32, 14e-3, 8, [0.25e6, 0.35e6],
+                           lambda X, Y: 1500 + 25 * np.exp(-((X - 2e-3) ** 2 + Y ** 2) / (2 * (4e-3) ** 2)), 12e-3)
+    ny, nx = p.shape
+    ocfg = o.OracleConfig(pml_m=p.pml_m, pml_strength=10, stencil_bounds=(1400, 1700), source_batch_size=4)
+    nf = p.frequencies_hz.size
+    n_tx, n_rx = p.tx_index.size, p.rx_index.size
+    dummy = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, p.frequencies_hz, np.zeros((n_tx, n_rx, nf)),
+                           np.ones((n_tx, n_rx, nf), bool))
+    Y = np.zeros((n_tx, n_rx, nf), complex)
+    for fi in range(nf):
+        u = o.make_solver(p.c_true, dummy, fi, ocfg).solve(o.point_sources(p.tx_index, range(n_tx), ny, nx))
+        Y[:, :, fi] = u.reshape(-1, n_tx, order="F")[p.rx_index - 1, :].T
+    obs = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, p.frequencies_hz, Y, np.ones((n_tx, n_rx, nf), bool))
+    schedule = [0, 0, 1, 1]
+    bounds, max_update, damping = (1400.0, 1700.0), 12.0, 1.0
+    # the FP64 oracle's loop
+    c = p.c_init.copy()
+    mask = p.update_mask
+    prev_z, prev_gz, direction, last = np.zeros_like(c), 0.0, np.zeros_like(c), None
+    for fi in schedule:
+        _, g, state = o.wust_oracle(c, obs, fi, ocfg, need_gradient=True, retain_state=True)
+        roi, z = o.roi_gradient(g, mask, p.x_m, p.y_m, 1500.0, p.frequencies_hz[fi], 0.0, 4)
+        direction, _, gz = o.ncg_direction(roi, z, prev_z, prev_gz, direction, fi == last)
+        prev_z, prev_gz, last = z, gz, fi
+        curvature = o.directional_curvature(state, direction, obs.rx_index, obs.mask[:, :, fi])
+        alpha = o.linearized_step_length(float(np.sum(roi * direction)), curvature)
+        c = o.project_slowness_update(c, direction, alpha, max_update, bounds, damping, mask)
+    # the device loop
+    cfg = dict(backend="gpu", bounds_mps=bounds, max_update_mps=max_update, step_damping=damping,
+               source_batch_size=4, pml_strength=10.0, pml_m=p.pml_m, stencil_bounds=(1400.0, 1700.0),
+               wavenumber="continuum", filter_cutoff=0.0, filter_order=4, update_mask=mask.astype(float),
+               frequency_schedule_hz=[p.frequencies_hz[k] for k in schedule], precision=precision)
+    out = wust_reconstruct(_gpu_obs(obs), p.c_init, cfg)
+    POOL.clear()
+    rms = float(np.sqrt(np.mean((out["c_mps"] - c) ** 2)))
+    assert float(np.sqrt(np.mean((c - p.c_init) ** 2))) > 1.0
+    assert rms < 0.05, rms
