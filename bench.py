@@ -206,6 +206,86 @@ def generate_observations(p, solver_cls, torch):
     return Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, [FREQ], Y, mask)
 
 
+def run_precision(args, torch):
+    """The precision study (config 3) as a report: config 1's geometry and
+    phantom (224^2, 32 TX, 128 RX) at twelve frequencies from 0.3 to 1.2 MHz
+    (3.1 points per wavelength at 1.2 MHz), observations from the FP64 oracle
+    on the true model.  Per profile and frequency, at the initial model: the
+    refinement's correction solves and the relative errors of the pressure
+    fields, the misfit and the gradient against the FP64 oracle; then a
+    continuation of three NCG updates per frequency and the RMS of the final
+    sound speed against the plain c64 run and against the true model.  One
+    JSON line per profile."""
+    from oracle import helmholtz_fp64 as o
+    from waveforminversionust_b200 import synthetic
+    from waveforminversionust_b200.objective import POOL, Observations, default_config, wust_oracle
+    from waveforminversionust_b200.reconstruct import wust_reconstruct
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    freqs = np.linspace(0.3e6, 1.2e6, 12)
+    p = synthetic.config1(seed=0, freqs=freqs)
+    ny, nx = p.shape
+    n_tx, n_rx, nf = p.tx_index.size, p.rx_index.size, freqs.size
+    ocfg = o.OracleConfig(pml_m=p.pml_m, pml_strength=10, stencil_bounds=(1400, 1700), source_batch_size=n_tx)
+    ones = np.ones((n_tx, n_rx, nf), bool)
+    dummy = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, freqs, np.zeros((n_tx, n_rx, nf)), ones)
+    src = o.point_sources(p.tx_index, range(n_tx), ny, nx)
+    Y = np.zeros((n_tx, n_rx, nf), complex)
+    for fi in range(nf):
+        u = o.make_solver(p.c_true, dummy, fi, ocfg).solve(src)
+        Y[:, :, fi] = u.reshape(-1, n_tx, order="F")[p.rx_index - 1, :].T
+    obs_o = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, freqs, Y, ones)
+    obs = Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, freqs, Y, ones)
+    ref = []
+    for fi in range(nf):
+        sv = o.make_solver(p.c_init, obs_o, fi, ocfg)
+        loss, g, _ = o.wust_oracle(p.c_init, obs_o, fi, ocfg, need_gradient=True, solver=sv)
+        ref.append((sv.solve(src), loss, g))
+
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    profiles = [("c64", "default"), ("c64-refined", "default"), ("tf32-refined", "default"), ("tf32-refined", "same")]
+    finals = {}
+    for prec, corr in profiles:
+        rows = []
+        for fi, f in enumerate(freqs):
+            s = HelmholtzSolver(p.x_m, p.y_m, p.c_init, None, f, -1, 10.0, p.pml_m,
+                                dict(backend="gpu", stencil_bounds=(1400, 1700)), precision=prec, max_sources=n_tx,
+                                correction_precision=corr)
+            u = s.solve(src.astype(np.complex64)).cpu().numpy()
+            st = s.stats()
+            s.close()
+            cfg = default_config(pml_m=p.pml_m, precision=prec, source_batch_size=n_tx, correction_precision=corr)
+            loss, g = wust_oracle(p.c_init, obs, fi, cfg, nargout=2)
+            u_ref, loss_ref, g_ref = ref[fi]
+            rows.append(dict(f_mhz=round(f / 1e6, 4), corrections=st["refine_iters"],
+                             pressure_err=rel(u[1:-1, 1:-1], u_ref[1:-1, 1:-1]),
+                             misfit_err=abs(loss - loss_ref) / loss_ref, gradient_err=rel(g, g_ref)))
+        POOL.clear()
+        rcfg = dict(backend="gpu", bounds_mps=(1300.0, 1800.0), max_update_mps=12.0, step_damping=1.0,
+                    source_batch_size=n_tx, pml_strength=10.0, pml_m=p.pml_m, stencil_bounds=(1400.0, 1700.0),
+                    wavenumber="continuum", filter_cutoff=0.0, filter_order=4, update_mask=p.update_mask.astype(float),
+                    frequency_schedule_hz=[f for f in freqs for _ in range(3)], precision=prec,
+                    correction_precision=corr)
+        t0 = time.perf_counter()
+        out = wust_reconstruct(obs, p.c_init, rcfg)
+        t_rec = time.perf_counter() - t0
+        POOL.clear()
+        name = prec if corr == "default" else f"{prec} (TF32 corrections)"
+        finals[name] = out["c_mps"]
+        print(json.dumps(dict(mode="precision", profile=name, workload="config1 geometry (224^2, 32 TX, 128 RX ring) "
+                              "at 12 frequencies 0.3-1.2 MHz, FP64-oracle observations", per_frequency=rows,
+                              max_pressure_err=max(r["pressure_err"] for r in rows),
+                              max_misfit_err=max(r["misfit_err"] for r in rows),
+                              max_gradient_err=max(r["gradient_err"] for r in rows),
+                              corrections=[r["corrections"] for r in rows],
+                              continuation=dict(updates=len(rcfg["frequency_schedule_hz"]), seconds=round(t_rec, 2),
+                                                rms_vs_c64_mps=float(np.sqrt(np.mean((out["c_mps"] - finals["c64"]) ** 2))),
+                                                rms_vs_true_mps=float(np.sqrt(np.mean((out["c_mps"] - p.c_true) ** 2))),
+                                                rms_initial_vs_true_mps=float(np.sqrt(np.mean((p.c_init - p.c_true) ** 2)))))),
+              flush=True)
+
+
 def run_dtft(args, torch):
     """The DTFT of the RF preparation (wust_dtft): 2048-sample float32 RF of
     256 x 256 transmitter/receiver pairs at 16 frequencies, RF resident in
@@ -354,7 +434,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="c64,c64-refined", help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft"],
+    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision"],
                     help="solve: factor once, then time forward solves of all transmitters (kernel profiling); "
                          "ncg: time NCG updates of the reconstruction loop, update rules on the device and on the host; "
                          "dtft: time the RF preparation's DTFT")
@@ -385,6 +465,9 @@ def main():
 
     if args.mode == "dtft":
         run_dtft(args, torch)
+        return
+    if args.mode == "precision":
+        run_precision(args, torch)
         return
     p = make_problem(seed=rank)
     ny, nx = p.shape

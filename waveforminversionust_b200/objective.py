@@ -83,13 +83,15 @@ class _SolverPool:
         key = (obs.shape_yx, obs.x_m.tobytes(), obs.y_m.tobytes(), float(cfg["pml_m"]), float(cfg["pml_strength"]),
                tuple(map(float, cfg["stencil_bounds"])), cfg.get("precision", "c64"),
                int(min(cfg.get("source_batch_size", 256), obs.n_tx)), float(cfg.get("refine_tol", 1e-5)),
-               None if not disp else (float(disp["time_step_s"]), float(disp["reference_speed_mps"])))
+               None if not disp else (float(disp["time_step_s"]), float(disp["reference_speed_mps"])),
+               cfg.get("correction_precision", "default"))
         f = float(obs.frequencies_hz[fi])
         s = self._pool.get(key)
         if s is None:
             s = HelmholtzSolver(obs.x_m, obs.y_m, c, None, f, -1, cfg["pml_strength"], cfg["pml_m"],
                                 dict(backend="gpu", stencil_bounds=cfg["stencil_bounds"], dispersion=disp),
-                                precision=cfg.get("precision", "c64"), max_sources=key[7], refine_tol=key[8])
+                                precision=cfg.get("precision", "c64"), max_sources=key[7], refine_tol=key[8],
+                                correction_precision=key[10])
             s.generation = 0
             self._pool[key] = s
         else:

@@ -28,7 +28,7 @@ from .objective import POOL, Observations, directional_curvature, wust_oracle
 _REQUIRED = ("backend", "bounds_mps", "max_update_mps", "step_damping", "source_batch_size", "pml_strength", "pml_m",
              "stencil_bounds", "wavenumber", "filter_cutoff", "filter_order", "update_mask")
 _ALLOWED = _REQUIRED + ("dispersion", "frequency_schedule_hz", "max_updates", "save_history",
-                        "evaluate_final_residual", "precision", "ncg_device")
+                        "evaluate_final_residual", "precision", "ncg_device", "correction_precision")
 
 
 def _prepare(obs: Observations, initial, cfg: dict) -> dict:

@@ -81,9 +81,11 @@ def _problem(name, interior, pml, dx, n_elem, radius, n_tx, freqs, c_true, mask_
                    c_init=np.full((n, n), 1500.0), update_mask=mask)
 
 
-def config1(seed: int = 0) -> Problem:
+def config1(seed: int = 0, freqs=None) -> Problem:
     """192^2 + 16-cell PML, dx 0.4 mm, 0.5 MHz, 128-element ring r = 35 mm, 32 TX,
-    three seeded elliptical inclusions (semi-axes 3-10 mm, 1450-1600 m/s)."""
+    three seeded elliptical inclusions (semi-axes 3-10 mm, 1450-1600 m/s).
+    ``freqs`` replaces the single 0.5 MHz (the precision study runs config 1's
+    geometry at twelve frequencies from 0.3 to 1.2 MHz)."""
     rng = np.random.default_rng(seed)
 
     def c_true(X, Y):
@@ -97,7 +99,8 @@ def config1(seed: int = 0) -> Problem:
             c[(xr / a) ** 2 + (yr / b) ** 2 < 1] = rng.uniform(1450, 1600)
         return c
 
-    return _problem("config1", 192, 16, 0.4e-3, 128, 35e-3, 32, [0.5e6], c_true, 30e-3)
+    return _problem("config1", 192, 16, 0.4e-3, 128, 35e-3, 32, [0.5e6] if freqs is None else list(freqs), c_true,
+                    30e-3)
 
 
 def config2(seed: int = 0, freqs=None) -> Problem:
