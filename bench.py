@@ -286,6 +286,78 @@ def run_precision(args, torch):
               flush=True)
 
 
+def run_autograd(args, torch):
+    """The differentiation check (config 4) as a report: 256^2 interior + 16-cell
+    PML (288^2), dx 0.3 mm, 128-element ring, 64 transmitters, 0.4 and 0.8 MHz,
+    observations from the FP64 oracle on the true model.  The slowness is
+    float32, 1/1500 s/m with a 2 % smooth random perturbation.  Per profile and
+    frequency, through ``torch.autograd`` over Phi_f(s) (backward = the adjoint
+    solve and slowness gradient of the same call): the misfit and gradient
+    against the FP64 oracle, the directional derivative along a smooth random
+    direction against central differences at relative steps 1e-3 .. 1e-6 (the
+    perturbed slowness formed in FP64), and the Gauss-Newton directional
+    curvature against the oracle's.  Refinement target 1e-10 so the central
+    differences resolve their step."""
+    from oracle import helmholtz_fp64 as o
+    from waveforminversionust_b200 import synthetic
+    from waveforminversionust_b200.autograd import curvature, misfit, misfit_and_state
+    from waveforminversionust_b200.objective import POOL, Observations, default_config
+    p = synthetic.config4(seed=0)
+    ny, nx = p.shape
+    freqs = p.frequencies_hz
+    n_tx, n_rx, nf = p.tx_index.size, p.rx_index.size, freqs.size
+    ocfg = o.OracleConfig(pml_m=p.pml_m, pml_strength=10, stencil_bounds=(1400, 1700), source_batch_size=n_tx)
+    ones = np.ones((n_tx, n_rx, nf), bool)
+    dummy = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, freqs, np.zeros((n_tx, n_rx, nf)), ones)
+    src = o.point_sources(p.tx_index, range(n_tx), ny, nx)
+    Y = np.zeros((n_tx, n_rx, nf), complex)
+    for fi in range(nf):
+        u = o.make_solver(p.c_true, dummy, fi, ocfg).solve(src)
+        Y[:, :, fi] = u.reshape(-1, n_tx, order="F")[p.rx_index - 1, :].T
+    obs_o = o.Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, freqs, Y, ones)
+    obs = Observations(p.x_m, p.y_m, p.tx_index, p.rx_index, freqs, Y, ones)
+    rng = np.random.default_rng(1)
+    s32 = ((1.0 + 0.02 * synthetic._smooth_noise(rng, (ny, nx), 6.0)) / 1500.0).astype(np.float32)
+    s64 = s32.astype(np.float64)
+    direction = synthetic._smooth_noise(rng, (ny, nx), 10.0) * p.update_mask * 1e-2 * float(np.abs(s64).max())
+    ref = []
+    for fi in range(nf):
+        loss, g, state = o.wust_oracle(1.0 / s64, obs_o, fi, ocfg, need_gradient=True, retain_state=True)
+        ref.append((loss, g, o.directional_curvature(state, direction, obs_o.rx_index, obs_o.mask[:, :, fi])))
+
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    d_dev = torch.as_tensor(direction, device="cuda")
+    for prec in ("c64-refined", "tf32-refined"):
+        cfg = default_config(pml_m=p.pml_m, precision=prec, source_batch_size=n_tx, refine_tol=1e-10)
+        rows = []
+        for fi in range(nf):
+            s0 = torch.tensor(s32, device="cuda", requires_grad=True)
+            loss = misfit(s0, obs, fi, cfg)
+            loss.backward()
+            g = s0.grad.to(torch.float64)
+            adj = float((g * d_dev).sum())
+            fds = {}
+            for rel_step in (1e-3, 1e-4, 1e-5, 1e-6):
+                h = rel_step * float(np.abs(s64).max()) / float(np.abs(direction).max())
+                with torch.no_grad():
+                    base = torch.as_tensor(s64, device="cuda")
+                    lp = float(misfit(base + h * d_dev, obs, fi, cfg))
+                    lm = float(misfit(base - h * d_dev, obs, fi, cfg))
+                fds[f"{rel_step:.0e}"] = abs((lp - lm) / (2 * h) - adj) / abs(adj)
+            _, _, state = misfit_and_state(torch.as_tensor(s64, device="cuda"), obs, fi, cfg)
+            kappa = curvature(state, direction)
+            loss_ref, g_ref, kappa_ref = ref[fi]
+            rows.append(dict(f_mhz=float(freqs[fi]) / 1e6, misfit_err=abs(loss.item() - loss_ref) / loss_ref,
+                             gradient_err=rel(g.cpu().numpy(), g_ref), directional_fd_rel_err=fds,
+                             curvature_err=abs(kappa - kappa_ref) / kappa_ref))
+            POOL.clear()
+        print(json.dumps(dict(mode="autograd", profile=prec, workload="config4: 256^2 + 16-cell PML, dx 0.3 mm, "
+                              "128-element ring, 64 TX, 0.4/0.8 MHz, float32 slowness with a 2 % smooth perturbation",
+                              refine_tol=1e-10, per_frequency=rows)), flush=True)
+
+
 def run_dtft(args, torch):
     """The DTFT of the RF preparation (wust_dtft): 2048-sample float32 RF of
     256 x 256 transmitter/receiver pairs at 16 frequencies, RF resident in
@@ -434,7 +506,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="c64,c64-refined", help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision"],
+    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision", "autograd"],
                     help="solve: factor once, then time forward solves of all transmitters (kernel profiling); "
                          "ncg: time NCG updates of the reconstruction loop, update rules on the device and on the host; "
                          "dtft: time the RF preparation's DTFT")
@@ -468,6 +540,9 @@ def main():
         return
     if args.mode == "precision":
         run_precision(args, torch)
+        return
+    if args.mode == "autograd":
+        run_autograd(args, torch)
         return
     p = make_problem(seed=rank)
     ny, nx = p.shape
