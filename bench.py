@@ -358,6 +358,97 @@ def run_autograd(args, torch):
                               refine_tol=1e-10, per_frequency=rows)), flush=True)
 
 
+def batch_problems(seed: int = 0, count: int = 24):
+    """Config 5's mix of independent inversions: interior grids from
+    {128, 192, 256, 384, 512}^2, PML 16-20 cells, dx 0.25-0.4 mm, ring arrays of
+    64-256 elements, 16-256 transmitters, each problem at its own frequency in
+    0.3-1.2 MHz, a seeded smooth phantom; the homogeneous 1500 m/s start."""
+    from waveforminversionust_b200 import synthetic
+    rng = np.random.default_rng(seed)
+    probs = []
+    for k in range(count):
+        interior = int(rng.choice([128, 192, 256, 384, 512]))
+        pml = int(rng.integers(16, 21))
+        dx = float(rng.uniform(0.25e-3, 0.4e-3))
+        radius = 0.42 * interior * dx
+        n_elem = int(min(rng.choice([64, 128, 256]), 2 ** int(np.log2(2 * np.pi * radius / (1.5 * dx)))))
+        n_tx = int(min(rng.choice([16, 32, 64, 128, 256]), n_elem))
+        f = float(rng.uniform(0.3e6, 1.2e6))
+        amp, sig = float(rng.uniform(10, 40)), float(rng.uniform(0.1, 0.3)) * interior * dx
+        probs.append(synthetic._problem(f"batch{k}", interior, pml, dx, n_elem, radius, n_tx, [f],
+                                        lambda X, Y, a=amp, w=sig: 1500 + a * np.exp(-(X ** 2 + Y ** 2) / (2 * w * w)),
+                                        0.9 * radius))
+    return probs
+
+
+class _GradientRun:
+    """One problem's gradient through the C ABI with device-resident inputs
+    (refactor + wust_solver_oracle with the gradient), on a given stream."""
+
+    def __init__(self, p, stream, torch, precision):
+        from waveforminversionust_b200 import _lib
+        from waveforminversionust_b200.solver import HelmholtzSolver
+        self.lib, self.check, self.need = _lib.load(), _lib.check, _lib.NEED_GRADIENT
+        ny, nx = p.shape
+        self.n_tx, self.n_rx, self.f = p.tx_index.size, p.rx_index.size, float(p.frequencies_hz[0])
+        self.solver = HelmholtzSolver(p.x_m, p.y_m, p.c_init, None, self.f, -1, 10.0, p.pml_m,
+                                      dict(backend="gpu", stencil_bounds=(1400, 1700)), precision=precision,
+                                      max_sources=self.n_tx, stream=stream)
+        rng = np.random.default_rng(ny * 1000 + self.n_tx)
+        Y = (rng.standard_normal((self.n_tx, self.n_rx)) + 1j * rng.standard_normal((self.n_tx, self.n_rx))) * 1e-3
+        self.c = torch.as_tensor(np.asfortranarray(p.c_init).T.copy(), device="cuda")
+        self.tx = torch.as_tensor(p.tx_index.astype(np.int32), device="cuda")
+        self.rx = torch.as_tensor(p.rx_index.astype(np.int32), device="cuda")
+        self.Y = torch.as_tensor(np.asfortranarray(Y).T.astype(np.complex64).copy(), device="cuda")
+        self.m = torch.ones((self.n_rx, self.n_tx), dtype=torch.uint8, device="cuda")
+        self.g = torch.empty((nx, ny), dtype=torch.float64, device="cuda")
+        self.loss = C.c_double()
+
+    def run(self):
+        h = C.c_void_p(self.solver.handle)
+        self.check(self.lib.wust_solver_refactor(h, C.c_void_p(self.c.data_ptr()), None, C.c_double(self.f)))
+        self.check(self.lib.wust_solver_oracle(h, C.c_void_p(self.tx.data_ptr()), self.n_tx,
+                                               C.c_void_p(self.rx.data_ptr()), self.n_rx, C.c_void_p(self.Y.data_ptr()),
+                                               C.c_void_p(self.m.data_ptr()), self.n_tx, self.need,
+                                               C.byref(self.loss), C.c_void_p(self.g.data_ptr())))
+
+    def close(self):
+        self.solver.close()
+
+
+def run_batch(args, torch):
+    """Config 5: 24 independent inversions of uneven size, one gradient each
+    (tf32-refined), run one after another: each gradient is timed with CUDA
+    events on its solver's stream after a warm-up gradient, the aggregate is
+    24 / the sum of the gradient times, and the per-problem latency is listed.
+    The problems are not run concurrently: the factorization and the sweeps
+    are persistent kernels whose grid barriers need all their CTAs resident,
+    which two such launches sharing the GPU would not guarantee.  Solvers are
+    built outside the timed regions, one at a time."""
+    probs = batch_problems()
+    precision = args.precision
+    stream = torch.cuda.Stream()
+    seq = []
+    for p in probs:
+        r = _GradientRun(p, stream, torch, precision)
+        r.run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq.append(dict(grid=p.shape[0], n_tx=int(p.tx_index.size), n_rx=int(p.rx_index.size),
+                        f_mhz=round(float(p.frequencies_hz[0]) / 1e6, 3), ms=round(e0.elapsed_time(e1), 3)))
+        r.close()
+    t_seq = sum(x["ms"] for x in seq)
+    print(json.dumps(dict(mode="batch", precision=precision, problems=len(probs),
+                          workload="config5: 24 independent inversions, interiors {128..512}^2 + 16-20 PML, "
+                                   "dx 0.25-0.4 mm, 16-256 TX, one frequency each in 0.3-1.2 MHz",
+                          value=len(probs) / (t_seq * 1e-3), unit="gradients/s", total_ms=t_seq,
+                          per_problem=seq)), flush=True)
+
+
 def run_dtft(args, torch):
     """The DTFT of the RF preparation (wust_dtft): 2048-sample float32 RF of
     256 x 256 transmitter/receiver pairs at 16 frequencies, RF resident in
@@ -506,7 +597,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="c64,c64-refined", help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision", "autograd"],
+    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision", "autograd", "batch"],
                     help="solve: factor once, then time forward solves of all transmitters (kernel profiling); "
                          "ncg: time NCG updates of the reconstruction loop, update rules on the device and on the host; "
                          "dtft: time the RF preparation's DTFT")
@@ -543,6 +634,9 @@ def main():
         return
     if args.mode == "autograd":
         run_autograd(args, torch)
+        return
+    if args.mode == "batch":
+        run_batch(args, torch)
         return
     p = make_problem(seed=rank)
     ny, nx = p.shape
