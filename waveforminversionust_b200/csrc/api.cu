@@ -302,8 +302,12 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
         factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
     }
     if (s->precision == WUST_PRECISION_TF32_REFINED) {
-        tc_pack_invT(s->invT, s->ny, s->nx, s->tc_geom, s->tc_afwd, s->tc_aadj, st);
-        if (s->bf16_corrections) tc_pack_invT16(s->invT, s->ny, s->nx, s->ck_geom, s->tc_afwd16, s->tc_aadj16, st);
+        if (s->bf16_corrections && s->use_chunks && s->ck_geom.kc == s->tc_geom.kc && s->ck_geom.mt == s->tc_geom.mt)
+            tc_pack_invT_both(s->invT, s->ny, s->nx, s->ck_geom, s->tc_afwd, s->tc_aadj, s->tc_afwd16, s->tc_aadj16, st);
+        else {
+            tc_pack_invT(s->invT, s->ny, s->nx, s->tc_geom, s->tc_afwd, s->tc_aadj, st);
+            if (s->bf16_corrections) tc_pack_invT16(s->invT, s->ny, s->nx, s->ck_geom, s->tc_afwd16, s->tc_aadj16, st);
+        }
         if (s->use_chunks) tc_chunk_prepare(s->coefs64(), s->tc_afwd, s->tc_aadj, s->ck_geom, s->chunk_buffers(), st);
     }
     WUST_CUDA(cudaEventRecord(s->ev[2], st));

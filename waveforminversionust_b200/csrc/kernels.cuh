@@ -78,6 +78,10 @@ size_t tc_chunk_state_floats(int ny);
 // Composed propagators of the chunks of all four substitutions (after tc_pack_invT).
 void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t *aadj, const TcChunkGeom &g,
                       const TcChunkBuffers &b, cudaStream_t st);
+// invT pages -> the TF32 packed operands (as tc_pack_invT) and the BF16 ones
+// (as tc_pack_invT16) in one pass over the pages
+void tc_pack_invT_both(const float2 *invT, int ny, int nx, const TcChunkGeom &g, uint8_t *afwd, uint8_t *aadj,
+                       uint8_t *afwd16, uint8_t *aadj16, cudaStream_t st);
 // invT pages -> BF16 packed operands of invT_j and invT_j^H (g.page_bytes16 per page)
 void tc_pack_invT16(const float2 *invT, int ny, int nx, const TcChunkGeom &g, uint8_t *afwd16, uint8_t *aadj16,
                     cudaStream_t st);

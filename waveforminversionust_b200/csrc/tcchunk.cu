@@ -791,6 +791,64 @@ __global__ void pack_invT16_kernel(const float2 *__restrict__ invT, int ny, int 
     }
 }
 
+// Both packings in one pass: each thread reads the 32 complex values of its
+// row in a BF16 K chunk and their transposes once, and writes the BF16 chunk
+// and the two TF32 chunks (16 complex columns each) it covers, for invT_j
+// and invT_j^H.  Same layouts as pack_invT_kernel and pack_invT16_kernel.
+__global__ void pack_invT_both_kernel(const float2 *__restrict__ invT, int ny, int n, int mt, int kc, int kc16,
+                                      size_t page_bytes16, uint8_t *afwd, uint8_t *aadj, uint8_t *afwd16,
+                                      uint8_t *aadj16) {
+    const int i_s = threadIdx.x;
+    const int c16 = blockIdx.x, m = blockIdx.y, j = blockIdx.z;
+    const int i = m * 64 + (i_s & 63);
+    const bool imrow = i_s >= 64;
+    const size_t off16 = (size_t)j * page_bytes16 + ((size_t)m * kc16 + c16) * tc::kAChunk;
+    const float2 *page = invT + (size_t)j * ny * ny;
+#pragma unroll 2
+    for (int u = 0; u < 8; ++u) {                   // complex columns 4u .. 4u + 3 of the BF16 chunk
+        uint32_t wf[4], wa[4];
+        float vf[8], va[8];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int k = c16 * kCkRowsPerChunk16 + 4 * u + h;
+            float2 af = make_float2(0.f, 0.f), aa = af;
+            if (i < n && k < n) {
+                af = page[(size_t)(i + 1) + (size_t)ny * (k + 1)];                  // invT(i, k)
+                const float2 at = page[(size_t)(k + 1) + (size_t)ny * (i + 1)];     // invT(k, i)
+                aa = make_float2(at.x, -at.y);                                      // invT^H(i, k)
+            }
+            const float f0 = imrow ? af.y : af.x, f1 = imrow ? af.x : -af.y;
+            const float a0 = imrow ? aa.y : aa.x, a1 = imrow ? aa.x : -aa.y;
+            wf[h] = (uint32_t)tc::to_bf16_bits(f0) | ((uint32_t)tc::to_bf16_bits(f1) << 16);
+            wa[h] = (uint32_t)tc::to_bf16_bits(a0) | ((uint32_t)tc::to_bf16_bits(a1) << 16);
+            vf[2 * h] = tc::to_tf32(f0);
+            vf[2 * h + 1] = tc::to_tf32(f1);
+            va[2 * h] = tc::to_tf32(a0);
+            va[2 * h + 1] = tc::to_tf32(a1);
+        }
+        *reinterpret_cast<uint4 *>(afwd16 + off16 + tc::chunk_off16(i_s, 8 * u)) = make_uint4(wf[0], wf[1], wf[2], wf[3]);
+        *reinterpret_cast<uint4 *>(aadj16 + off16 + tc::chunk_off16(i_s, 8 * u)) = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+        const int c = 2 * c16 + u / 4;               // TF32 chunk of these columns
+        if (c < kc) {
+            const size_t off = (((size_t)j * mt + m) * kc + c) * tc::kAChunk;
+            const int ke = 8 * (u % 4);
+            *reinterpret_cast<float4 *>(afwd + off + tc::chunk_off(i_s, ke)) = make_float4(vf[0], vf[1], vf[2], vf[3]);
+            *reinterpret_cast<float4 *>(afwd + off + tc::chunk_off(i_s, ke + 4)) = make_float4(vf[4], vf[5], vf[6], vf[7]);
+            *reinterpret_cast<float4 *>(aadj + off + tc::chunk_off(i_s, ke)) = make_float4(va[0], va[1], va[2], va[3]);
+            *reinterpret_cast<float4 *>(aadj + off + tc::chunk_off(i_s, ke + 4)) = make_float4(va[4], va[5], va[6], va[7]);
+        }
+    }
+}
+
+void tc_pack_invT_both(const float2 *invT, int ny, int nx, const TcChunkGeom &g, uint8_t *afwd, uint8_t *aadj,
+                       uint8_t *afwd16, uint8_t *aadj16, cudaStream_t st) {
+    const dim3 grid(g.kc16, g.mt, nx);
+    pack_invT_both_kernel<<<grid, 128, 0, st>>>(invT, ny, g.n, g.mt, g.kc, g.kc16, g.page_bytes16, afwd, aadj, afwd16,
+                                                aadj16);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
 void tc_pack_invT16(const float2 *invT, int ny, int nx, const TcChunkGeom &g, uint8_t *afwd16, uint8_t *aadj16,
                     cudaStream_t st) {
     const dim3 grid(g.kc16, g.mt, nx);
