@@ -777,6 +777,20 @@ def main():
                         traffic / (head["sweep_ms_per_launch"] * 1e-3) / 1e9 if traffic else None),
                     algorithmic_flop_per_launch=flop,
                     launch_ms=head["sweep_ms_per_launch"] if flop == fl["apply"] else head["factor_ms"])
+    # the step by phase: factorization (assembly, Schur inverses, and for the
+    # TF32 profile the page packs and chunk propagators), the sweep pairs, and
+    # the rest (FP64 refinement launches, fit, gradient, host synchronisation);
+    # algorithmic flops against the tensor peak of the arithmetic used (TF32 is
+    # half the bf16 figure; the CUDA-core c64 path is shown against it as well)
+    tc_peak = peak_tf / 2 if args.precision == "tf32-refined" else peak_tf
+    rest_ms = head["ms_per_step"] - head["factor_ms"] - sweep_ms_step
+    phases = dict(
+        factorization=dict(ms=head["factor_ms"], algorithmic_tflops=fl["factor"] / (head["factor_ms"] * 1e-3) / 1e12,
+                           frac_of_tensor_peak=fl["factor"] / (head["factor_ms"] * 1e-3) / 1e12 / tc_peak),
+        sweep_pairs=dict(ms=sweep_ms_step, pairs=head["sweeps_per_step"],
+                         algorithmic_tflops=fl["apply"] / (head["sweep_ms_per_launch"] * 1e-3) / 1e12,
+                         frac_of_tensor_peak=fl["apply"] / (head["sweep_ms_per_launch"] * 1e-3) / 1e12 / tc_peak),
+        rest=dict(ms=rest_ms), tensor_peak_tflops=tc_peak)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(p, n_solves=8)
@@ -793,7 +807,8 @@ def main():
                 detail=dict(factor_ms=head["factor_ms"], refine_iters=head["refine_iters"],
                             sweep_ms_per_launch=head["sweep_ms_per_launch"], sweeps_per_step=head["sweeps_per_step"],
                             factor_stats=head["factor_stats"],
-                            final_relative_residual=head["final_residual"], flops=fl, variants=variants))
+                            final_relative_residual=head["final_residual"], flops=fl, phases=phases,
+                            variants=variants))
     if cpu:
         line["cpu_baseline"] = dict(value=cpu["value"], unit="gradients/s", cores=cpu["cores"], kind=cpu["kind"],
                                     sample=cpu["sample"])
