@@ -105,10 +105,17 @@ __device__ __forceinline__ bool on_ring(int y, int x, int ny, int nx) {
     return y == 0 || x == 0 || y == ny - 1 || x == nx - 1;
 }
 
+// One thread per grid point of a 32 x 8 tile, all sources in order (the sum
+// over s is the same at every point on every run).  The lambda tile with its
+// one-point halo is double-buffered in shared memory: the next source's
+// halo values and field value are loaded into registers while the current
+// source is computed, so each source costs one barrier and no exposed load.
 __global__ void __launch_bounds__(TY * TX) gradient_kernel(const float2 *u, const float2 *lam, const double2 *mult,
                                                            const double2 *scale, int ny, int nx, int nb, double d,
                                                            double e, double *grad) {
-    __shared__ float2 L[TX + 2][TY + 2];
+    constexpr int kHalo = (TY + 2) * (TX + 2);
+    constexpr int kPer = (kHalo + TY * TX - 1) / (TY * TX);    // halo entries per thread
+    __shared__ float2 L[2][TX + 2][TY + 2];
     const int ty = threadIdx.x % TY, tx = threadIdx.x / TY;
     const int y0 = blockIdx.x * TY, x0 = blockIdx.y * TX;
     const int y = y0 + ty, x = x0 + tx;
@@ -120,30 +127,60 @@ __global__ void __launch_bounds__(TY * TX) gradient_kernel(const float2 *u, cons
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b) w[a][b] = mass_w(a - 1, b - 1, d, e);
-    double acc = 0;
+    // this thread's halo entries: offset in a source plane, or -1 (outside the
+    // tile's halo, or on the Dirichlet ring, which the adjoint massApply zeroes
+    // before the convolution)
+    long long hoff[kPer];
+    int hl[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int q = threadIdx.x + TY * TX * k;
+        const int ly = q % (TY + 2), lx = q / (TY + 2);
+        const int gy = y0 + ly - 1, gx = x0 + lx - 1;
+        hl[k] = q < kHalo ? lx * (TY + 2) + ly : -1;
+        hoff[k] = (q < kHalo && gy > 0 && gx > 0 && gy < ny - 1 && gx < nx - 1) ? (long long)gy + (long long)ny * gx
+                                                                                 : -1;
+    }
     const size_t fs = (size_t)ny * nx;
+    float2 hv[kPer], uv = make_float2(0.f, 0.f);
+    auto fetch = [&](int s) {
+#pragma unroll
+        for (int k = 0; k < kPer; ++k)
+            hv[k] = hoff[k] >= 0 ? lam[fs * s + (size_t)hoff[k]] : make_float2(0.f, 0.f);
+        uv = inside ? u[fs * s + idx] : make_float2(0.f, 0.f);
+    };
+    auto stash = [&](int buf) {
+        float2 *Lb = &L[buf][0][0];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k)
+            if (hl[k] >= 0) Lb[hl[k]] = hv[k];
+    };
+    double acc = 0;
+    if (nb > 0) {
+        fetch(0);
+        stash(0);
+    }
+    float2 ucur = uv;
+    __syncthreads();
     for (int s = 0; s < nb; ++s) {
-        const float2 *ls = lam + fs * s;
-        for (int q = threadIdx.x; q < (TY + 2) * (TX + 2); q += TY * TX) {
-            const int ly = q % (TY + 2), lx = q / (TY + 2);
-            const int gy = y0 + ly - 1, gx = x0 + lx - 1;
-            // adjoint massApply zeroes the Dirichlet ring before the convolution
-            const bool ok = gy > 0 && gx > 0 && gy < ny - 1 && gx < nx - 1;
-            L[lx][ly] = ok ? ls[(size_t)gy + (size_t)ny * gx] : make_float2(0.f, 0.f);
-        }
-        __syncthreads();
+        const int cur = s & 1;
+        if (s + 1 < nb) fetch(s + 1);               // in flight during this source's arithmetic
         if (inside) {
             double2 ml = make_double2(0.0, 0.0);
 #pragma unroll
             for (int a = 0; a < 3; ++a)
 #pragma unroll
                 for (int b = 0; b < 3; ++b) {
-                    const float2 v = L[tx + b][ty + a];
+                    const float2 v = L[cur][tx + b][ty + a];
                     ml.x += w[a][b] * (double)v.x;
                     ml.y += w[a][b] * (double)v.y;
                 }
-            const double2 av = zmul(scale[s], zmul(m, z_from(u[fs * s + idx])));
+            const double2 av = zmul(scale[s], zmul(m, z_from(ucur)));
             acc -= av.x * ml.x + av.y * ml.y;    // -Re(conj(av) * ml)
+        }
+        if (s + 1 < nb) {
+            stash(cur ^ 1);                         // last read in the previous source, before its barrier
+            ucur = uv;
         }
         __syncthreads();
     }
