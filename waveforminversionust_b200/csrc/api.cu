@@ -168,6 +168,7 @@ struct wust_solver {
     }
     // Newton-Schulz factorization (TF32 profile)
     void *ns_scratch = nullptr;
+    int ns_head = 3;                  // pages inverted directly before the Newton-Schulz run (learned)
     NsGeom ns_g{};
     long long ns_stats[4] = {};       // GEMMs, X updates, Newton-Schulz pages, Gauss-Jordan pages
     float2 *stage_c = nullptr; size_t stage_c_cap = 0;
@@ -297,7 +298,8 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
         WUST_CUDA(cudaStreamSynchronize(st));
         check_assembly(astat0);
         for (long long &v : s->ns_stats) v = 0;
-        ns_factor(s->coefs64(), s->invT, s->ns_g, s->ns_scratch, s->fscratch, s->fscratch_bytes, st, s->ns_stats);
+        ns_factor(s->coefs64(), s->invT, s->ns_g, s->ns_scratch, s->fscratch, s->fscratch_bytes, st, s->ns_stats,
+                  &s->ns_head);
     } else {
         factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
     }

@@ -122,8 +122,11 @@ int ns_max_ctas();
 // the Gauss-Jordan kernel elsewhere (gj_scratch as for factor_launch).
 // stats (nullable, long long[4]): GEMMs, X updates, Newton-Schulz pages,
 // Gauss-Jordan pages (accumulated).
+// head_hint (in/out, may be null): the first page of the Newton-Schulz run
+// (at least 3); the pages before it go to one Gauss-Jordan launch.  Updated
+// from this factorization for the next one of the same solver.
 void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
-               size_t gj_scratch_bytes, cudaStream_t st, long long *stats);
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint);
 
 // ---- assemble.cu -----------------------------------------------------------
 struct AssemblyInput {

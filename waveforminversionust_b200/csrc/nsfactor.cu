@@ -763,7 +763,7 @@ __global__ void identity_page_kernel(Coefs<float2> co, float2 *invT, int j, int 
 }
 
 void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
-               size_t gj_scratch_bytes, cudaStream_t st, long long *stats) {
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint) {
     const int nx = co.nx;
     int hstat[3];
     auto gj = [&](int a, int b) {
@@ -789,14 +789,19 @@ void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_
         return h != 0;
     };
     // the first pages (Dirichlet column and the PML start) and the last one
-    // (Dirichlet column) have no usable predecessor
-    const int head = std::min(nx, 3);
-    if (g.ks <= 0 || nx <= head + 1) {
+    // (Dirichlet column) have no usable predecessor.  head_hint carries, from
+    // one factorization of a solver to the next, how far past them the
+    // iteration kept failing on the first page of each launch (the outer PML
+    // columns of this grid): those pages join the head's Gauss-Jordan launch.
+    const int base = std::min(nx, 3);
+    if (g.ks <= 0 || nx <= base + 1) {
         gj(0, nx);
         return;
     }
+    const int head = std::max(base, std::min(head_hint ? *head_hint : base, nx - 2));
     gj(identity(0) ? 1 : 0, head);
-    int j = head, fallbacks = 0;
+    int j = head, fallbacks = 0, learned = head;
+    bool leading = true;                        // every launch so far failed on its first page
     while (j < nx - 1) {
         if (fallbacks >= 16) {                  // not this operator's regime: finish with Gauss-Jordan
             gj(j, nx - 1);
@@ -804,6 +809,8 @@ void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_
             break;
         }
         const int bad = ns_launch(co, invT, g, (uint8_t *)ns_scratch, j, nx - 1, st, stats);
+        leading = leading && bad == j;
+        if (leading) learned = bad + 1;
         if (bad < 0) {
             j = nx - 1;
         } else {
@@ -812,6 +819,7 @@ void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_
             j = bad + 1;
         }
     }
+    if (head_hint) *head_hint = std::min(learned, base + 16);
     if (!identity(nx - 1)) gj(nx - 1, nx);
 }
 
