@@ -137,53 +137,75 @@ def make_problem(seed: int = 0):
     return synthetic.config2(seed=seed, freqs=[FREQ])
 
 
-def cpu_reference_sample(p, n_solves: int = 8) -> dict:
-    """FP64 sparse-LU gradient timed on a bounded sample and extrapolated."""
-    from oracle import helmholtz_fp64 as o
-    ny, nx = p.shape
-    t0 = time.perf_counter()
-    s = o.HelmholtzSolverFP64(p.x_m, p.y_m, p.c_init, np.zeros(p.shape), FREQ, -1, 10.0, p.pml_m,
-                              dict(backend="cpu", stencil_bounds=(1400, 1700)), factor=False)
-    t1 = time.perf_counter()
-    lu = o.spla.splu(s.H)
-    t2 = time.perf_counter()
-    src = o.point_sources(p.tx_index, range(n_solves), ny, nx).reshape(ny * nx, n_solves, order="F")
-    lu.solve(src)
-    t3 = time.perf_counter()
-    lu.solve(src, trans="H")
-    t4 = time.perf_counter()
-    per_fwd = (t3 - t2) / n_solves
-    per_adj = (t4 - t3) / n_solves
-    t_grad = (t1 - t0) + (t2 - t1) + N_TX * (per_fwd + per_adj)
-    return dict(value=1.0 / t_grad, unit="gradients/s", cores=1, kind="port",
-                sample=(f"FP64 sparse LU (SciPy SuperLU, 1 thread) at {ny}x{nx}: assembly {t1 - t0:.2f} s + "
-                        f"factor {t2 - t1:.2f} s + {n_solves} forward and {n_solves} adjoint solves "
-                        f"({per_fwd * 1e3:.0f}/{per_adj * 1e3:.0f} ms each), extrapolated to {N_TX}+{N_TX} solves"),
-                seconds_per_gradient=t_grad)
+PARITY_TX = [0, 37, 73, 110, 146, 183, 219, 255]
+
+
+def media(p) -> dict:
+    """Media a gradient is evaluated at: the homogeneous start of the first NCG
+    iteration, a textured NCG-like iterate halfway to the phantom (the
+    headline), and the phantom itself (the most textured medium)."""
+    return dict(homogeneous=p.c_init, halfway=0.5 * (p.c_init + p.c_true), phantom=p.c_true)
+
+
+HEADLINE_MEDIUM = "halfway"
+
+
+def thread_env() -> dict:
+    return {k: os.environ[k] for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
+            if k in os.environ}
+
+
+def cpu_gradient(pool, p, c, Y, mask, keep=()) -> dict:
+    """One full FP64 gradient (all transmitters; SuperLU per worker) on the host cores."""
+    return pool.gradient(p.x_m, p.y_m, c, FREQ, p.pml_m, p.tx_index, p.rx_index, Y, mask, keep_fields=keep)
+
+
+def cpu_sample_text(out) -> str:
+    return (f"one full FP64 gradient (all {N_TX} transmitters forward + adjoint, nothing extrapolated): "
+            f"SciPy SuperLU sparse LU in complex128, transmitters split over {out['workers']} spawned worker "
+            f"processes with one BLAS thread each, every worker assembling and factoring its own operator "
+            f"(factor {out['factor_seconds']:.1f} s, solves {out['solve_seconds']:.1f} s in the slowest worker)")
 
 
 def run_reference(args):
+    """The reference's CPU path for this workload (backend 'cpu' of
+    HelmholtzSolver: FP64 sparse LU; MATLAB's UMFPACK is unavailable here, so
+    the oracle port with SciPy SuperLU stands in), on all host cores: each
+    timed step is one full gradient over every transmitter.  Warm-up steps
+    run the same pool on the config-1 grid (224^2, 32 transmitters)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle.parallel_fp64 import ParallelOracle, host_cores
+    from waveforminversionust_b200 import synthetic
     p = make_problem()
-    for _ in range(args.warmup):
-        cpu_reference_sample(p, n_solves=2)
-    vals = []
-    t0 = time.perf_counter()
-    last = None
-    for _ in range(args.steps):
-        last = cpu_reference_sample(p, n_solves=4)
-        vals.append(last["value"])
-    wall = time.perf_counter() - t0
-    v = float(np.mean(vals))
+    c_eval = media(p)[HEADLINE_MEDIUM]
+    small = synthetic.config1(seed=0)
+    with ParallelOracle() as pool:
+        Y = pool.observe(p.x_m, p.y_m, p.c_true, FREQ, p.pml_m, p.tx_index, p.rx_index)
+        mask = np.ones(Y.shape, bool)
+        Ys = pool.observe(small.x_m, small.y_m, small.c_true, 0.5e6, small.pml_m, small.tx_index, small.rx_index)
+        for _ in range(args.warmup):
+            pool.gradient(small.x_m, small.y_m, small.c_init, 0.5e6, small.pml_m, small.tx_index, small.rx_index,
+                          Ys, np.ones(Ys.shape, bool))
+        secs = []
+        last = None
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            last = cpu_gradient(pool, p, c_eval, Y, mask)
+            secs.append(last["seconds"])
+        wall = time.perf_counter() - t0
+    ms = 1e3 * wall / args.steps
+    v = 1e3 / ms
     line = dict(impl="reference", metric="gradients_per_second", value=v, unit="gradients/s", n_gpus=args.gpus,
-                steps=args.steps, warmup=args.warmup, ms_per_step=1e3 / v, higher_is_better=True, scaling="weak",
+                steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="c128", data="synthetic",
-                config=dict(workload=WORKLOADS[WORKLOAD]["text"], global_batch=N_TX),
-                cpu_baseline=dict(value=v, unit="gradients/s", cores=1, kind="port", sample=last["sample"]),
+                config=dict(workload=WORKLOADS[WORKLOAD]["text"], global_batch=N_TX, medium=HEADLINE_MEDIUM),
+                cpu_baseline=dict(value=v, unit="gradients/s", cores=last["workers"], kind="port",
+                                  sample=cpu_sample_text(last)),
                 e2e=dict(value=v, unit="gradients/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
-                wall_seconds=wall)
+                host=dict(cpu_count=os.cpu_count(), affinity_cores=host_cores(), thread_env=thread_env()),
+                seconds_per_step=secs, wall_seconds=wall)
     print(json.dumps(line), flush=True)
 
 
@@ -649,20 +671,19 @@ def main():
         return
     fl = flops_per_gradient(ny, nx, N_TX)
     stream = torch.cuda.current_stream()
+    M = media(p)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-
-    def measure(precision: str, with_e2e: bool):
-        cfg = default_config(pml_m=p.pml_m, precision=precision, source_batch_size=N_TX)
-        solver = HelmholtzSolver(p.x_m, p.y_m, p.c_init, None, FREQ, -1, 10.0, p.pml_m,
+    def measure(precision: str, c_model, with_e2e: bool, parity: bool = False):
+        solver = HelmholtzSolver(p.x_m, p.y_m, c_model, None, FREQ, -1, 10.0, p.pml_m,
                                  dict(backend="gpu", stencil_bounds=(1400, 1700)), precision=precision,
                                  max_sources=N_TX, stream=stream)
         h = C.c_void_p(solver.handle)
-        c_dev = torch.as_tensor(np.asfortranarray(p.c_init).T.copy(), device="cuda")   # (nx, ny) == col-major
+        c_dev = torch.as_tensor(np.asfortranarray(c_model).T.copy(), device="cuda")   # (nx, ny) == col-major
         tx_dev = torch.as_tensor(obs.tx_index.astype(np.int32), device="cuda")
         rx_dev = torch.as_tensor(obs.rx_index.astype(np.int32), device="cuda")
         Y_dev = torch.as_tensor(np.asfortranarray(obs.Y[:, :, 0]).T.astype(np.complex64).copy(), device="cuda")
@@ -677,7 +698,7 @@ def main():
                                               N_TX, _lib.NEED_GRADIENT, C.byref(loss), C.c_void_p(g_dev.data_ptr())))
 
         # host buffers for e2e (pinned, as a caller would keep them)
-        c_h = torch.as_tensor(np.asfortranarray(p.c_init).T.copy()).pin_memory()
+        c_h = torch.as_tensor(np.asfortranarray(c_model).T.copy()).pin_memory()
         tx_h = np.ascontiguousarray(obs.tx_index.astype(np.int32))
         rx_h = np.ascontiguousarray(obs.rx_index.astype(np.int32))
         Y_h = torch.as_tensor(np.asfortranarray(obs.Y[:, :, 0]).T.astype(np.complex64).copy()).pin_memory()
@@ -715,6 +736,15 @@ def main():
                    loss=loss.value, clocks=clk.summary(),
                    sweep_ms_per_launch=(sw_ms1 - sw_ms0) / max(sw_n1 - sw_n0, 1),
                    sweeps_per_step=(sw_n1 - sw_n0) / args.steps, factor_stats=solver.factor_stats())
+        if parity:
+            # the timed call's outputs, and the forward fields of 8 transmitters
+            # from a 256-source solve of the same solver (outside the timed region)
+            res["gradient"] = g_dev.cpu().numpy().T.copy()
+            src = torch.zeros((N_TX, nx, ny), dtype=torch.complex64, device="cuda")
+            src.view(N_TX, -1)[torch.arange(N_TX, device="cuda"), torch.as_tensor(p.tx_index - 1, device="cuda")] = 1
+            u = solver.solve(src.permute(2, 1, 0))
+            res["fields"] = u[:, :, PARITY_TX].cpu().numpy().astype(np.complex128)
+            del src, u
         if with_e2e:
             for _ in range(2):
                 step_host()
@@ -735,10 +765,17 @@ def main():
         solver.close()
         return res
 
-    head = measure(args.precision, with_e2e=True)
+    want_cpu = rank == 0 and world == 1 and not args.no_cpu_baseline
+    head = measure(args.precision, M[HEADLINE_MEDIUM], with_e2e=True, parity=want_cpu)
+    other_media = {}
+    for name in M:
+        if name != HEADLINE_MEDIUM:
+            r = measure(args.precision, M[name], with_e2e=False)
+            other_media[name] = dict(ms_per_step=r["ms_per_step"], value=r["value"], factor_ms=r["factor_ms"],
+                                     refine_iters=r["refine_iters"], factor_stats=r["factor_stats"])
     variants = {}
     for v in [x for x in args.variants.split(",") if x and x != args.precision]:
-        variants[v] = measure(v, with_e2e=False)
+        variants[v] = measure(v, M[HEADLINE_MEDIUM], with_e2e=False)
         variants[v].pop("clocks", None)
 
     peaks = {}
@@ -757,7 +794,7 @@ def main():
         flop = fl["apply"]
         achieved = flop / (head["sweep_ms_per_launch"] * 1e-3) / 1e12
         kname = ("tc_chunk_kernel (column-chunked tcgen05 block-LU sweep pairs, 256 sources, 3 launches per "
-                 "substitution; mean over the step's pairs: 2 TF32 solves + 4 BF16 correction solves)"
+                 "substitution; mean over the step's pairs: 2 TF32 solves + BF16 correction solves)"
                  if args.precision == "tf32-refined" else "sweep kernels (CUDA-core block-LU sweep pair)")
     else:
         flop = fl["factor"]
@@ -767,10 +804,12 @@ def main():
     # DRAM bytes of one sweep pair of the dominant kernel (its six launches),
     # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one
     # pass) at 552^2 with 256 sources: TF32 pair 12.48 GB read + 1.19 GB
-    # written, BF16 correction pair 8.27 + 1.16 GB; the step runs 2 + 4
+    # written, BF16 correction pair 8.27 + 1.16 GB; weighted by the step's
+    # 2 TF32 pairs and (pairs - 2) BF16 pairs
     traffic = None
     if flop == fl["apply"] and args.precision == "tf32-refined" and WORKLOAD == "config2":
-        traffic = (2 * 13.67e9 + 4 * 9.42e9) / 6
+        n_pairs = max(head["sweeps_per_step"], 2.0)
+        traffic = (2 * 13.67e9 + (n_pairs - 2) * 9.42e9) / n_pairs
     roofline = dict(kernel=kname, bound="tensor", achieved=achieved, peak=peak_tf, unit="TFLOP/s",
                     frac=achieved / peak_tf, peak_source=peak_src, traffic=traffic,
                     traffic_unit="bytes per launch (ncu)", hbm_gbs_achieved=(
@@ -791,15 +830,33 @@ def main():
                          algorithmic_tflops=fl["apply"] / (head["sweep_ms_per_launch"] * 1e-3) / 1e12,
                          frac_of_tensor_peak=fl["apply"] / (head["sweep_ms_per_launch"] * 1e-3) / 1e12 / tc_peak),
         rest=dict(ms=rest_ms), tensor_peak_tflops=tc_peak)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_sample(p, n_solves=8)
+    cpu = parity = None
+    if want_cpu:
+        from oracle.parallel_fp64 import ParallelOracle, host_cores
+        with ParallelOracle() as pool:
+            out = cpu_gradient(pool, p, M[HEADLINE_MEDIUM], obs.Y[:, :, 0], obs.mask[:, :, 0], keep=PARITY_TX)
+        cpu = dict(value=1.0 / out["seconds"], unit="gradients/s", cores=out["workers"], kind="port",
+                   sample=cpu_sample_text(out),
+                   host=dict(cpu_count=os.cpu_count(), affinity_cores=host_cores(), thread_env=thread_env()))
+        want_u = np.stack([out["fields"][k] for k in PARITY_TX], axis=2)
+
+        def rel(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+        parity = dict(
+            reference="FP64 sparse LU (SciPy SuperLU, complex128) on the same medium and observations",
+            medium=HEADLINE_MEDIUM,
+            misfit_rel_err=abs(head["loss"] - out["loss"]) / out["loss"],
+            gradient_rel_err=rel(head["gradient"], out["gradient"]),
+            pressure_rel_err=rel(head["fields"], want_u),
+            pressure_rel_err_per_tx=[rel(head["fields"][:, :, k], want_u[:, :, k]) for k in range(len(PARITY_TX))],
+            pressure_tx=PARITY_TX,
+            targets=dict(pressure=1e-5, gradient=1e-4))
     line = dict(metric="gradients_per_second", value=head["value"], unit="gradients/s", n_gpus=world,
                 steps=args.steps, warmup=args.warmup, ms_per_step=head["ms_per_step"], higher_is_better=True,
                 scaling="weak", vs_baseline=None,
                 dtype={"c64": "c64", "c64-refined": "c64+c128-refine"}.get(args.precision, "tf32+c128-refine"),
                 data="synthetic",
-                config=dict(workload=WORKLOADS[WORKLOAD]["text"],
+                config=dict(workload=WORKLOADS[WORKLOAD]["text"], medium=HEADLINE_MEDIUM,
                             global_batch=N_TX * world, precision=args.precision, parallelism=f"replicas{world}",
                             l2="inputs larger than L2 (invT 1.35 GB, fields 0.62 GB)"),
                 e2e=head["e2e"], gpu_launches=int(round(head["launches_per_step"] * args.steps)),
@@ -808,10 +865,13 @@ def main():
                             sweep_ms_per_launch=head["sweep_ms_per_launch"], sweeps_per_step=head["sweeps_per_step"],
                             factor_stats=head["factor_stats"],
                             final_relative_residual=head["final_residual"], flops=fl, phases=phases,
-                            variants=variants))
+                            media=dict({HEADLINE_MEDIUM: dict(ms_per_step=head["ms_per_step"], value=head["value"],
+                                                              factor_ms=head["factor_ms"],
+                                                              refine_iters=head["refine_iters"],
+                                                              factor_stats=head["factor_stats"])}, **other_media),
+                            variants=variants, parity=parity))
     if cpu:
-        line["cpu_baseline"] = dict(value=cpu["value"], unit="gradients/s", cores=cpu["cores"], kind=cpu["kind"],
-                                    sample=cpu["sample"])
+        line["cpu_baseline"] = cpu
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

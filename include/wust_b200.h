@@ -101,9 +101,10 @@ int wust_decomp_block_lu(const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 
  * device array that every GPU loading the library holds until process exit.
  * Ny must not exceed WUST_NOALLOC_MAX_NY (larger grids: WUST_ERR_INVALID_INPUT).
  * All calls share that array, so calls that overlap on the GPU race; callers
- * must serialize them.  The first call on each device looks up the array's
- * address with that device current; make it before any stream capture.
- * No timing output. */
+ * must serialize them.  Every call looks up the array's address with the
+ * caller's device current (so a device reset between calls is safe); the
+ * first call on a device may load the module, so make it before any stream
+ * capture.  No timing output. */
 int wust_decomp_block_lu_noalloc(const wust_c64 *Ld, const wust_c64 *Ll, const wust_c64 *Lu,
                                  const wust_c64 *Dd, const wust_c64 *Dl, const wust_c64 *Du,
                                  const wust_c64 *Ud, const wust_c64 *Ul, const wust_c64 *Uu,

@@ -56,6 +56,10 @@ def test_reference_arm_line_fields():
     assert line["impl"] == "reference" and line["metric"] == "gradients_per_second" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    # measured in full on the host cores, and the host is described
+    assert line["cpu_baseline"]["cores"] >= 1 and "nothing extrapolated" in line["cpu_baseline"]["sample"]
+    assert line["host"]["cpu_count"] >= line["host"]["affinity_cores"] >= 1
+    assert abs(line["ms_per_step"] * line["steps"] - 1e3 * line["wall_seconds"]) < 1e-6 * line["ms_per_step"]
 
 
 def test_batch_problem_mix_follows_the_configuration():

@@ -3,9 +3,11 @@
 Hosts that own the device heap (MATLAB's gpuArray manager, framework caching
 allocators) or that cannot pay cudaMalloc's device synchronization use this
 entry point; its scratch is a static device array, so it allocates nothing.
-The test calls it through the C ABI twice in a row on different operators
-and checks each result against the allocating entry point
-(wust_decomp_block_lu) with the tolerance the factor parity tests use.
+The tests call it through the C ABI twice in a row on different operators
+and once at its largest grid, and check each result against the allocating
+entry point (wust_decomp_block_lu) with the tolerance the factor parity
+tests use; the largest-grid test also checks that the device's free memory
+does not change across a call.
 The file name makes pytest collect it last.
 """
 import ctypes as C
@@ -60,6 +62,48 @@ def test_noalloc_matches_allocating_entry_point_twice():
         assert np.all(np.isfinite(got))
         err = np.linalg.norm(got - want) / np.linalg.norm(want)
         assert err < 2e-5
+
+
+def _dominant_blocks(ny, nx, seed):
+    """A diagonally dominant block-tridiagonal operator in the reference's
+    nine block shapes (every Schur page well conditioned)."""
+    rng = np.random.default_rng(seed)
+
+    def c(shape, scale, offset=0.0):
+        return offset + scale * (rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+    return dict(Dd=c((ny, nx), 0.1, 4.0), Dl=c((ny - 1, nx), 0.2, -1.0), Du=c((ny - 1, nx), 0.2, -1.0),
+                Ld=c((ny, nx - 1), 0.1, -0.5), Ll=c((ny - 1, nx - 1), 0.05), Lu=c((ny - 1, nx - 1), 0.05),
+                Ud=c((ny, nx - 1), 0.1, -0.5), Ul=c((ny - 1, nx - 1), 0.05), Uu=c((ny - 1, nx - 1), 0.05))
+
+
+def test_noalloc_at_its_largest_grid_matches_and_allocates_nothing():
+    """At Ny = WUST_NOALLOC_MAX_NY the static scratch is used to its last
+    byte; the result must still match the allocating entry point, and the
+    device's free memory must not move across a call (nothing allocated)."""
+    import torch
+    from waveforminversionust_b200 import _lib
+    lib = _lib.load()
+    ny, nx = 1024, 3
+    coefs = _dominant_blocks(ny, nx, seed=11)
+    rc, want = _factor(lib, lib.wust_decomp_block_lu, coefs, noalloc=False)
+    assert rc == 0, lib.wust_last_error().decode()
+    dev = [_device_colmajor(coefs[n]) for n in NAMES]
+    invT = torch.full((nx, ny, ny), complex(np.nan, np.nan), dtype=torch.complex64, device="cuda")
+    args = [C.c_void_p(t.data_ptr()) for t in dev] + [ny, nx, C.c_void_p(invT.data_ptr()), None]
+    assert lib.wust_decomp_block_lu_noalloc(*args) == 0, lib.wust_last_error().decode()   # warm-up
+    torch.cuda.synchronize()
+    invT.fill_(complex(np.nan, np.nan))
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    rc = lib.wust_decomp_block_lu_noalloc(*args)
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert rc == 0, lib.wust_last_error().decode()
+    assert free_after == free_before, (free_before, free_after)
+    got = invT.cpu().numpy()
+    assert np.all(np.isfinite(got))
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < 2e-5
 
 
 def test_noalloc_rejects_grids_beyond_its_limit():

@@ -382,11 +382,9 @@ void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t 
     p.timeout_ns = (unsigned long long)(timeout_s * 1e9);
     WUST_CUDA(cudaMemsetAsync(tail, 0, 8 * sizeof(int), stream));
 
-    static bool configured = false;
-    if (!configured) {
-        WUST_CUDA(cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmemBytes));
-        configured = true;
-    }
+    // Set on every launch: the attribute belongs to the current device's
+    // context, which a caller may switch or reset between calls.
+    WUST_CUDA(cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmemBytes));
     int dev = 0, sms = 0, per_sm = 0;
     WUST_CUDA(cudaGetDevice(&dev));
     WUST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

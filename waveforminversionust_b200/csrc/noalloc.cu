@@ -20,11 +20,12 @@
 //     rewritten before they are read.  Two calls whose work overlaps on the
 //     GPU (different streams, or host threads without ordering) race on the
 //     array and corrupt each other's results; callers must serialize them.
-//   * The first call on each device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current.  That lookup may load
-//     the module, so make the first call outside of any stream capture.
-#include <mutex>
-
+//   * Every call looks up the array's device address (cudaGetSymbolAddress)
+//     with the caller's device current, so a device reset between calls (a
+//     host such as MATLAB can reset the GPU, which reloads the module,
+//     possibly at another address) never leaves a stale pointer behind.  The
+//     lookup allocates nothing, but the first one on a device may load the
+//     module: make the first call on each device outside any stream capture.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -36,22 +37,14 @@ constexpr size_t kNoallocScratchBytes = (factor_scratch_bytes_for(kNoallocMaxNy)
 
 static __device__ __align__(256) unsigned char g_factor_scratch[kNoallocScratchBytes];
 
-static std::mutex g_noalloc_mutex;
-static void *g_noalloc_addr[64] = {};
-
-// Device address of g_factor_scratch on the current device (looked up once per device).
+// Device address of g_factor_scratch in the current device's context.  In
+// host code the symbol names a host-side shadow, so kernels must be given
+// this address, never &g_factor_scratch.
 static void *noalloc_scratch_address() {
-    int dev = 0;
-    WUST_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) fail(WUST_ERR_RUNTIME, "device ordinal %d out of range for the static scratch table", dev);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-        void *ptr = nullptr;
-        WUST_CUDA(cudaGetSymbolAddress(&ptr, g_factor_scratch));
-        if (!ptr) fail(WUST_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
-        g_noalloc_addr[dev] = ptr;
-    }
-    return g_noalloc_addr[dev];
+    void *ptr = nullptr;
+    WUST_CUDA(cudaGetSymbolAddress(&ptr, g_factor_scratch));
+    if (!ptr) fail(WUST_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
+    return ptr;
 }
 
 static bool noalloc_device_pointer(const void *p) {

@@ -667,13 +667,11 @@ NsGeom ns_geom(int ny, int max_ctas) {
 }
 
 int ns_max_ctas() {
-    static thread_local int configured_device = -1;
     int dev = 0, sms = 0, per_sm = 0;
     WUST_CUDA(cudaGetDevice(&dev));
-    if (configured_device != dev) {
-        WUST_CUDA(cudaFuncSetAttribute(ns_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNsSmem));
-        configured_device = dev;
-    }
+    // the attribute lives in the current device's context (set every time: a
+    // caller may switch devices or reset one between calls)
+    WUST_CUDA(cudaFuncSetAttribute(ns_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNsSmem));
     WUST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     WUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ns_factor_kernel, kNsThreads, kNsSmem));
     return sms * per_sm;

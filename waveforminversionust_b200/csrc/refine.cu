@@ -368,14 +368,9 @@ __global__ void __launch_bounds__(kRfThreads, 2) refine_kernel(const RefineParam
 
 template <bool ADJ, int MODE>
 void refine_launch_one(const RefineParams &p, dim3 grid, size_t smem, cudaStream_t st) {
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    WUST_CUDA(cudaGetDevice(&dev));
-    if (configured_device != dev) {
-        WUST_CUDA(cudaFuncSetAttribute(refine_kernel<ADJ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)refine_smem_bytes(kRfRows)));
-        configured_device = dev;
-    }
+    // per launch: the attribute lives in the current device's context
+    WUST_CUDA(cudaFuncSetAttribute(refine_kernel<ADJ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)refine_smem_bytes(kRfRows)));
     refine_kernel<ADJ, MODE><<<grid, kRfThreads, smem, st>>>(p);
 }
 

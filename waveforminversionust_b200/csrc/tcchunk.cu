@@ -858,15 +858,12 @@ void tc_pack_invT16(const float2 *invT, int ny, int nx, const TcChunkGeom &g, ui
 }
 
 static void ck_configure() {
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    WUST_CUDA(cudaGetDevice(&dev));
-    if (configured_device == dev) return;
+    // called before every launch: the attribute lives in the current
+    // device's context, which a caller may switch or reset between calls
     WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
     WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
     WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
     WUST_CUDA(cudaFuncSetAttribute(tc_chunk_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCkSmem));
-    configured_device = dev;
 }
 
 int tc_chunk_max_ctas() {

@@ -538,13 +538,9 @@ static void configure_one() {
                                    (int)kSweepSmem));
 }
 static void configure_all() {
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    WUST_CUDA(cudaGetDevice(&dev));
-    if (configured_device == dev) return;
+    // before every launch: the attribute lives in the current device's context
     configure_one<false, 1>(); configure_one<false, 2>(); configure_one<false, 4>();
     configure_one<true, 1>(); configure_one<true, 2>(); configure_one<true, 4>();
-    configured_device = dev;
 }
 
 int tc_sweep_max_ctas() {
