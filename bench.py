@@ -197,6 +197,7 @@ def run_reference(args):
         wall = time.perf_counter() - t0
     ms = 1e3 * wall / args.steps
     v = 1e3 / ms
+    ref_gpu = reference_gpu_c64(p, c_eval)
     line = dict(impl="reference", metric="gradients_per_second", value=v, unit="gradients/s", n_gpus=args.gpus,
                 steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="c128", data="synthetic",
@@ -206,7 +207,79 @@ def run_reference(args):
                 e2e=dict(value=v, unit="gradients/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
                 host=dict(cpu_count=os.cpu_count(), affinity_cores=host_cores(), thread_env=thread_env()),
                 seconds_per_step=secs, wall_seconds=wall)
+    if ref_gpu:
+        line["reference_gpu_c64"] = ref_gpu
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_c64(p, c, repeats: int = 3) -> dict | None:
+    """The reference's GPU path on this device, beside its CPU path: the
+    nine-point blocks assembled on the host in FP64 and cast to complex single
+    (HelmholtzSolver.m:112-113, 152-160), then the reference's own MEX kernels
+    -- decompBlockLU (pivoted cuSOLVER LU per Schur page) and applyBlockLU
+    (cuBLAS Cgemm3m sweeps), forward over all transmitters and adjoint over
+    as many receiver-residual sources -- compiled unchanged and called through
+    the MEX runtime stand-in.  The source fit and gradient (MATLAB gpuArray
+    element-wise code in the reference) are not included.  None when no GPU is
+    present or the kernels were not built."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        from oracle import helmholtz_fp64 as o
+        from oracle.mexshim import driver
+        if not driver.reference_available():
+            return None
+    except Exception:
+        return None
+    rt = driver.runtime()
+    ker = driver.reference_kernels()
+    ny, nx = p.shape
+
+    def colmajor(a, dtype=torch.complex64):
+        t = torch.as_tensor(np.ascontiguousarray(np.asarray(a).T)).to(device="cuda", dtype=dtype)
+        return rt.gpu(t.permute(*reversed(range(t.dim()))), dims=np.asarray(a).shape)
+
+    names = ("Ld", "Ll", "Lu", "Dd", "Dl", "Du", "Ud", "Ul", "Uu")
+    src = torch.zeros((N_TX, nx, ny), dtype=torch.complex64, device="cuda")
+    src.view(N_TX, -1)[torch.arange(N_TX, device="cuda"), torch.as_tensor(p.tx_index - 1, device="cuda")] = 1
+    rng = np.random.default_rng(0)
+    res = torch.zeros_like(src)
+    vals = rng.standard_normal((N_TX, p.rx_index.size)) + 1j * rng.standard_normal((N_TX, p.rx_index.size))
+    res.view(N_TX, -1)[:, torch.as_tensor(p.rx_index - 1, device="cuda")] = torch.as_tensor(
+        vals.astype(np.complex64), device="cuda")
+    src_mx = rt.gpu(src.permute(2, 1, 0), dims=(ny, nx, N_TX))
+    res_mx = rt.gpu(res.permute(2, 1, 0), dims=(ny, nx, N_TX))
+    rows = []
+    for rep in range(repeats + 1):
+        t0 = time.perf_counter()
+        pf = o.pml_fields(p.x_m, p.y_m, c, np.zeros(p.shape), FREQ, -1, 10.0, p.pml_m)
+        b, d, e = o.stencil_opt_params(1400.0, 1700.0, FREQ, pf.h, pf.g)
+        coefs = o.nine_point_coefficients(pf.A, pf.B, pf.C, pf.k, b, d, e, pf.h, pf.g, nx, ny)
+        blocks = [colmajor(coefs[n]) for n in names]
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        inv, info = rt.call(ker["decompBlockLU"], 2, *blocks)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        lu = [blocks[i] for i in (0, 1, 2, 6, 7, 8)]
+        (u,) = rt.call(ker["applyBlockLU"], 1, src_mx, *lu, inv, rt.logical(False))
+        t3 = time.perf_counter()
+        del u
+        (lam,) = rt.call(ker["applyBlockLU"], 1, res_mx, *lu, inv, rt.logical(True))
+        t4 = time.perf_counter()
+        del lam, inv
+        if rep:
+            rows.append(dict(assembly_ms=1e3 * (t1 - t0), factor_ms=1e3 * (t2 - t1),
+                             factor_gpu_ms=info.field("total_gpu_ms").scalar(), forward_ms=1e3 * (t3 - t2),
+                             adjoint_ms=1e3 * (t4 - t3)))
+    med = {k: float(np.median([r[k] for r in rows])) for k in rows[0]}
+    core = med["factor_ms"] + med["forward_ms"] + med["adjoint_ms"]
+    return dict(kind="the reference's MEX kernels compiled unchanged from Runtime/solver/decompBlockLU.cu and "
+                     "applyBlockLU.cu (cuSOLVER getrf/getrs per Schur page, cuBLAS Cgemm3m sweeps), called through "
+                     "the MEX runtime stand-in on the same GPU; blocks assembled on the host in FP64",
+                repeats=repeats, **med, kernels_ms=core, gradients_per_second_kernels=1e3 / core,
+                gradients_per_second_with_assembly=1e3 / (core + med["assembly_ms"]))
 
 
 def generate_observations(p, solver_cls, torch):
