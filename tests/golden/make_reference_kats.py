@@ -6,7 +6,9 @@ Sources (read as text; the reference is MATLAB and cannot run here):
   Runtime/tests/test_runtime.m:22-28,185-188  projection of 1500 m/s by a
       crossing direction with alpha 1 -> 1512 m/s inside the mask
 When the reference tree is present, the script checks that each literal
-still appears in test_runtime.m before writing.
+still appears in test_runtime.m before writing.  The tree's location is the
+first command-line argument, else the WUST_REFERENCE_ROOT environment
+variable, else /root/reference.
 
 The stencil_opt_params entry is an oracle regression value (no reference
 output exists for it); it guards the restatement against drift.
@@ -19,7 +21,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-REF_TEST = "/root/reference/Runtime/tests/test_runtime.m"
+REF_ROOT = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WUST_REFERENCE_ROOT", "/root/reference"))
+REF_TEST = os.path.join(REF_ROOT, "Runtime", "tests", "test_runtime.m")
 
 NCG = [
     # [d, beta, gz] = wust_ncg_direction([1; 2], [2; 1], [1; .5], 1.5, [-1; -2], true)
