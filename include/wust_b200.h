@@ -215,6 +215,17 @@ int wust_solver_oracle(wust_solver *s, const int32_t *tx_index, int n_tx,
  * (directional_curvature.m:1-26).  direction: ny x nx double. */
 int wust_solver_curvature(wust_solver *s, const double *direction, double *curvature);
 
+/* No counterpart in the reference (its NCG loop needs only the scalar
+ * curvature of directional_curvature.m).  The Gauss-Newton Hessian-vector
+ * product of the misfit along a direction, with the source scales frozen as
+ * directional_curvature.m:1-26 freezes them, on the state kept by the last
+ * oracle call with WUST_RETAIN_STATE:
+ *     q = J d = -a (H^{-1} M (v .* d))(rx) .* mask,   out = Re(J^H q),
+ * i.e. one more forward and one more adjoint solve, reusing the factors.
+ * direction, out: ny x nx double (host or device); curvature (nullable)
+ * receives d' out = ||q||^2, the value wust_solver_curvature returns. */
+int wust_solver_gauss_newton_product(wust_solver *s, const double *direction, double *out, double *curvature);
+
 /* The NCG update of wust_reconstruct (wust_reconstruct.m:24-57) on the GPU,
  * FP64, for hosts that keep the model, gradient and direction in device
  * memory between oracle calls (the reference runs these rules in MATLAB on

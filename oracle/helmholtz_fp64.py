@@ -21,6 +21,8 @@ reference's Helmholtz path (WaveformInversionUST, MATLAB + MEX):
                                 complex128 (same recursion and sweeps, any dtype)
 * ``wust_oracle``               Runtime/matlab/wust_oracle.m:1-86
 * ``directional_curvature``     Runtime/matlab/directional_curvature.m:1-26
+* ``gauss_newton_product``      Re(J^H J d): the product behind directional_curvature.m's
+                                quadratic form (its J d, wust_oracle.m:62-68's J^H)
 * NCG scalars                   Runtime/matlab/wust_ncg_direction.m, linearized_step_length.m,
                                 wust_roi_gradient.m, wust_project_slowness_update.m
 * ``ringing_removal_filt``      Runtime/solver/ringingRemovalFilt.m:1-45
@@ -590,6 +592,36 @@ def directional_curvature(state, direction, rx_index, receiver_mask):
         deriv = -uf[rx0, :] * a[None, :] * receiver_mask[ids, :].T
         curvature += float(np.sum(np.abs(deriv) ** 2))
     return curvature
+
+
+def gauss_newton_product(state, direction, rx_index, receiver_mask):
+    """Re(J^H J d) with the source scales frozen: the Hessian-vector product
+    whose quadratic form d' (J^H J d) is directional_curvature.m:1-26.
+
+    J d is the curvature's ``derivative`` (directional_curvature.m:14-19);
+    J^H q is the adjoint solve and accumulation of the oracle's gradient
+    (wust_oracle.m:62-68) with q in place of the residual.  Returns
+    (product, curvature)."""
+    solver = state["solver"]
+    ny, nx = direction.shape
+    out = np.zeros((ny, nx))
+    curvature = 0.0
+    offset = 0
+    rx0 = np.asarray(rx_index) - 1
+    for v, a in zip(state["virtual"], state["scales"]):
+        nb = a.size
+        ids = list(range(offset, offset + nb))
+        offset += nb
+        source = solver.mass_apply(v * direction[:, :, None], adjoint=False)
+        uf = solver.solve(source, adjoint=False).reshape(-1, nb, order="F")
+        q = -uf[rx0, :] * a[None, :] * receiver_mask[ids, :].T
+        curvature += float(np.sum(np.abs(q) ** 2))
+        rhs = np.zeros((ny * nx, nb), np.complex128)
+        rhs[rx0, :] = q
+        lam = solver.solve(rhs.reshape(ny, nx, nb, order="F"), adjoint=True)
+        lam = solver.mass_apply(lam, adjoint=True)
+        out += np.sum(-np.real(np.conj(v * a[None, None, :]) * lam), axis=2)
+    return out, curvature
 
 
 # ---------------------------------------------------------------------------

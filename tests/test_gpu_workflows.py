@@ -178,3 +178,44 @@ def test_reconstruction_final_sound_speed_matches_oracle(precision):
     rms = float(np.sqrt(np.mean((out["c_mps"] - c) ** 2)))
     assert float(np.sqrt(np.mean((c - p.c_init) ** 2))) > 1.0
     assert rms < 0.05, rms
+
+
+def test_autograd_forward_only_and_gauss_newton_products(ref_fixture):
+    """The Function on a device slowness: without requires_grad it runs the
+    forward solve only (fewer sweeps, same misfit); with create_graph its
+    gradient is differentiable and torch.autograd gives the Gauss-Newton
+    Hessian-vector product, matching the FP64 oracle's and reproducing
+    directional_curvature as its quadratic form."""
+    import torch
+    from oracle import helmholtz_fp64 as o
+    from waveforminversionust_b200.autograd import misfit
+    from waveforminversionust_b200.objective import POOL, default_config
+    fx = ref_fixture
+    obs = _gpu_obs(fx["obs"])
+    cfg = default_config(pml_m=.004, pml_strength=10, source_batch_size=3, precision="c64-refined", refine_tol=1e-10)
+    s = torch.tensor(1 / fx["initial"], dtype=torch.float64, device="cuda")
+    l0 = misfit(s, obs, 0, cfg)                         # no gradient wanted: forward only
+    solver = next(iter(POOL._pool.values()))
+    n0 = solver.sweep_times()[1]
+    l1 = misfit(s, obs, 0, cfg)
+    pairs_forward = solver.sweep_times()[1] - n0
+    s1 = s.clone().requires_grad_(True)
+    n0 = solver.sweep_times()[1]
+    l2 = misfit(s1, obs, 0, cfg)
+    pairs_gradient = solver.sweep_times()[1] - n0
+    assert float(l0) == float(l1) and abs(float(l2) - float(l1)) <= 1e-12 * float(l1)
+    assert 0 < pairs_forward < pairs_gradient, (pairs_forward, pairs_gradient)
+    (g,) = torch.autograd.grad(l2, s1, create_graph=True)
+    assert g.is_cuda
+    d = torch.tensor(fx["direction"], dtype=torch.float64, device="cuda")
+    e = torch.roll(d, 3, dims=1) * torch.tensor(fx["mask"], dtype=torch.float64, device="cuda")
+    (hd,) = torch.autograd.grad(g, s1, d, retain_graph=True)
+    (he,) = torch.autograd.grad(g, s1, e)
+    _, g_ref, state = o.wust_oracle(fx["initial"], fx["obs"], 0, fx["cfg"], retain_state=True)
+    hd_ref, k_ref = o.gauss_newton_product(state, fx["direction"], fx["obs"].rx_index, fx["obs"].mask[:, :, 0])
+    assert np.linalg.norm(g.detach().cpu().numpy() - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+    hd_np = hd.cpu().numpy()
+    assert np.linalg.norm(hd_np - hd_ref) <= 1e-5 * np.linalg.norm(hd_ref)
+    assert abs(float((d * hd).sum()) - k_ref) <= 1e-5 * k_ref
+    assert abs(float((e * hd).sum()) - float((d * he).sum())) <= 1e-6 * abs(float((d * hd).sum()))
+    POOL.clear()

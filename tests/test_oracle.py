@@ -157,3 +157,20 @@ def test_stencil_params_against_golden():
     b, d, e = o.stencil_opt_params(*k["args"])
     assert b == 5 / 6
     assert abs(d - k["d"]) < 1e-12 and abs(e - k["e"]) < 1e-12
+
+
+def test_gauss_newton_product_is_the_curvature_form(ref_fixture):
+    """The oracle's Gauss-Newton product Re(J^H J d): its quadratic form is
+    directional_curvature.m's curvature and it is symmetric."""
+    from oracle import helmholtz_fp64 as o
+    fx = ref_fixture
+    _, _, state = o.wust_oracle(fx["initial"], fx["obs"], 0, fx["cfg"], retain_state=True)
+    mask = fx["obs"].mask[:, :, 0]
+    d = fx["direction"]
+    e = np.roll(d, 3, axis=1) * fx["mask"]
+    hd, kappa = o.gauss_newton_product(state, d, fx["obs"].rx_index, mask)
+    he, _ = o.gauss_newton_product(state, e, fx["obs"].rx_index, mask)
+    k_ref = o.directional_curvature(state, d, fx["obs"].rx_index, mask)
+    assert abs(kappa - k_ref) <= 1e-12 * k_ref
+    assert abs(float(np.sum(d * hd)) - k_ref) <= 1e-9 * k_ref
+    assert abs(float(np.sum(e * hd)) - float(np.sum(d * he))) <= 1e-9 * abs(float(np.sum(d * hd)))

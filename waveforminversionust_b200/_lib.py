@@ -30,7 +30,7 @@ EXPORTED = (
     "wust_decomp_block_lu", "wust_decomp_block_lu_noalloc", "wust_apply_block_lu",
     "wust_solver_create", "wust_solver_refactor", "wust_solver_destroy", "wust_solver_timings",
     "wust_solver_stencil", "wust_solver_block", "wust_solver_solve", "wust_solver_mass_apply",
-    "wust_solver_oracle", "wust_solver_curvature", "wust_ncg_roi_gradient", "wust_ncg_direction",
+    "wust_solver_oracle", "wust_solver_curvature", "wust_solver_gauss_newton_product", "wust_ncg_roi_gradient", "wust_ncg_direction",
     "wust_ncg_dot", "wust_ncg_project", "wust_dtft", "wust_solver_stats", "wust_solver_factor_stats", "wust_solver_sweep_times",
     "wust_selftest_barrier_timeout",
 )
@@ -88,6 +88,7 @@ def load() -> C.CDLL:
     lib.wust_solver_mass_apply.argtypes = [vp, vp, i, i, vp]
     lib.wust_solver_oracle.argtypes = [vp, vp, i, vp, i, vp, vp, i, i, pd, vp]
     lib.wust_solver_curvature.argtypes = [vp, vp, pd]
+    lib.wust_solver_gauss_newton_product.argtypes = [vp, vp, vp, pd]
     d = C.c_double
     lib.wust_ncg_roi_gradient.argtypes = [vp, vp, vp, d, d, d, d, vp, vp]
     lib.wust_ncg_direction.argtypes = [vp, vp, vp, vp, d, C.c_int, vp, pd, pd]

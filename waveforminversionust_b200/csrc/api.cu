@@ -923,6 +923,49 @@ int wust_solver_curvature(wust_solver *s, const double *direction, double *curva
     });
 }
 
+int wust_solver_gauss_newton_product(wust_solver *s, const double *direction, double *out, double *curvature) {
+    return guarded([&] {
+        if (!s || !direction || !out) fail(WUST_ERR_INVALID_INPUT, "Gauss-Newton product arguments missing");
+        if (!s->ret_valid) fail(WUST_ERR_INVALID_INPUT, "no retained oracle state (call the oracle with WUST_RETAIN_STATE)");
+        const long long t0 = g_kernel_launches;
+        cudaStream_t st = s->st;
+        const size_t N = s->plane();
+        WUST_CUDA(cudaMemcpyAsync(s->dir, direction, N * sizeof(double), cudaMemcpyDefault, st));
+        WUST_CUDA(cudaMemsetAsync(s->grad, 0, N * sizeof(double), st));
+        const int n_tx = s->ret_ntx, n_rx = s->ret_nrx;
+        const int bs = s->smax;
+        for (int first = 0; first < n_tx; first += bs) {
+            const int nb = std::min(bs, n_tx - first);
+            const float2 *uf = s->ret_u + N * first;
+            // J d: the linearized forward solve of directional_curvature.m
+            curvature_source_launch(uf, s->mult, s->dir, s->work, s->ny, s->nx, nb, s->d, s->e, st);
+            SrcView sv{};
+            sv.mode = SRC_DENSE;
+            sv.dense = s->work;
+            solve_into(s, sv, nb, false, s->u);
+            linearized_residual_launch(s->u, s->rx_lin, s->maskd, s->scale + first, n_tx, n_rx, first, nb, s->ny,
+                                       s->nx, s->resid, s->loss_src + first, st);
+            // Re(J^H q): the oracle's adjoint solve and gradient accumulation on q
+            SrcView adj{};
+            adj.mode = SRC_SCATTER;
+            adj.at = s->rx_at;
+            adj.vals = s->resid;
+            adj.n_slots = n_rx;
+            solve_into(s, adj, nb, true, s->lam);
+            gradient_launch(uf, s->lam, s->mult, s->scale + first, s->ny, s->nx, nb, s->d, s->e, s->grad, st);
+        }
+        std::vector<double> part(n_tx);
+        WUST_CUDA(cudaMemcpyAsync(part.data(), s->loss_src, n_tx * sizeof(double), cudaMemcpyDeviceToHost, st));
+        WUST_CUDA(cudaMemcpyAsync(out, s->grad, N * sizeof(double), cudaMemcpyDefault, st));
+        WUST_CUDA(cudaStreamSynchronize(st));
+        double k = 0;
+        for (double v : part) k += v;
+        if (!std::isfinite(k)) fail(WUST_ERR_NUMERICAL_FAILURE, "Nonfinite curvature");
+        if (curvature) *curvature = k;
+        s->launches = g_kernel_launches - t0;
+    });
+}
+
 // ---------------------------------------------------------------------------
 // NCG update on the device (wust_reconstruct.m:24-57)
 // ---------------------------------------------------------------------------

@@ -175,6 +175,12 @@ void curvature_source_launch(const float2 *u, const double2 *mult, const double 
 void curvature_reduce_launch(const float2 *u, const int32_t *rx_lin, const uint8_t *mask, const double2 *scale,
                              int n_tx, int n_rx, int first_tx, int nb, int ny, int nx, double *out,
                              cudaStream_t st);
+// q(r, s) = -a_s u_s(rx_r) on unmasked receivers (zero elsewhere) into
+// resid[r + n_rx s], the linearized residual J d of the Gauss-Newton
+// product, and sum_r |q|^2 per source into out[s]
+void linearized_residual_launch(const float2 *u, const int32_t *rx_lin, const uint8_t *mask, const double2 *scale,
+                                int n_tx, int n_rx, int first_tx, int nb, int ny, int nx, float2 *resid, double *out,
+                                cudaStream_t st);
 // virt = mult .* u
 void virtual_source_launch(const float2 *u, const double2 *mult, float2 *virt, int ny, int nx, int n,
                            cudaStream_t st);

@@ -280,6 +280,39 @@ void curvature_reduce_launch(const float2 *u, const int32_t *rx_lin, const uint8
     WUST_LAUNCH_CHECK();
 }
 
+// The linearized residual of the Gauss-Newton product (source scales frozen,
+// directional_curvature.m:12-20): q = J d = -a (H^{-1} M (v .* d))(rx) .* mask,
+// written as the adjoint right-hand side of J^H q, with ||q||^2 per source.
+__global__ void __launch_bounds__(FIT_THREADS) linearized_residual_kernel(const float2 *u, const int32_t *rx_lin,
+                                                                          const uint8_t *mask, const double2 *scale,
+                                                                          int n_tx, int n_rx, int first_tx, int ny,
+                                                                          int nx, float2 *resid, double *out) {
+    __shared__ double sh[FIT_THREADS / 32];
+    const int s = blockIdx.x, t = first_tx + s;
+    const float2 *us = u + (size_t)ny * nx * s;
+    double acc = 0;
+    for (int r = threadIdx.x; r < n_rx; r += FIT_THREADS) {
+        double2 q = make_double2(0.0, 0.0);
+        if (mask[t + (size_t)n_tx * r]) {
+            const double2 v = zmul(z_from(us[rx_lin[r]]), scale[s]);
+            q = make_double2(-v.x, -v.y);
+            acc += zabs2(q);
+        }
+        resid[r + (size_t)n_rx * s] = c_from(q);
+    }
+    acc = block_sum<FIT_THREADS>(acc, sh);
+    if (threadIdx.x == 0) out[s] = acc;
+}
+
+void linearized_residual_launch(const float2 *u, const int32_t *rx_lin, const uint8_t *mask, const double2 *scale,
+                                int n_tx, int n_rx, int first_tx, int nb, int ny, int nx, float2 *resid, double *out,
+                                cudaStream_t st) {
+    linearized_residual_kernel<<<nb, FIT_THREADS, 0, st>>>(u, rx_lin, mask, scale, n_tx, n_rx, first_tx, ny, nx,
+                                                           resid, out);
+    ++g_kernel_launches;
+    WUST_LAUNCH_CHECK();
+}
+
 __global__ void virtual_source_kernel(const float2 *u, const double2 *mult, float2 *virt, size_t plane, size_t total) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
         virt[i] = c_from(zmul(mult[i % plane], z_from(u[i])));

@@ -128,28 +128,38 @@ def wust_oracle(c, obs: Observations, fi: int, cfg: dict, nargout: int = 2, solv
     """Source-projected least squares at frequency ``fi`` (0-based).
 
     ``nargout`` follows wust_oracle.m:5-6: 1 -> loss, 2 -> (loss, gradient),
-    3 -> (loss, gradient, state for ``directional_curvature``).
+    3 -> (loss, gradient, state for ``directional_curvature``).  A CUDA
+    tensor ``c`` stays on the device and the gradient comes back as a CUDA
+    float64 tensor [ny, nx]; otherwise both are host NumPy arrays.
     """
     need_gradient = nargout > 1
     retain = nargout > 2
     ny, nx = obs.shape_yx
+    on_device = isinstance(c, torch.Tensor) and c.is_cuda
+    if not on_device:
+        c = np.asarray(c, np.float64)
     if solver is None:
-        solver = POOL.get(np.asarray(c, np.float64), obs, fi, cfg)
+        solver = POOL.get(c, obs, fi, cfg)
     lib = _lib.load()
     tx = np.ascontiguousarray(obs.tx_index, dtype=np.int32)
     rx = np.ascontiguousarray(obs.rx_index, dtype=np.int32)
     Y = _host_c(obs.Y[:, :, fi], np.complex64)
     mask = _host_c(obs.mask[:, :, fi], np.uint8)
     loss = C.c_double()
-    grad = np.zeros((ny, nx), order="F") if need_gradient else None
+    grad = None
+    if need_gradient:
+        # column-major [y, x]: a contiguous [x, y] tensor on the device
+        grad = torch.empty((nx, ny), dtype=torch.float64, device="cuda") if on_device else np.zeros((ny, nx), order="F")
+    gptr = None if grad is None else C.c_void_p(grad.data_ptr() if on_device else grad.ctypes.data)
     flags = (_lib.NEED_GRADIENT if need_gradient else 0) | (_lib.RETAIN_STATE if retain else 0)
     bs = int(cfg.get("source_batch_size") or obs.n_tx)
     check(lib.wust_solver_oracle(C.c_void_p(solver.handle), tx.ctypes.data_as(C.c_void_p), tx.size,
                                  rx.ctypes.data_as(C.c_void_p), rx.size, Y.ctypes.data_as(C.c_void_p),
-                                 mask.ctypes.data_as(C.c_void_p), bs, flags, C.byref(loss),
-                                 None if grad is None else grad.ctypes.data_as(C.c_void_p)))
+                                 mask.ctypes.data_as(C.c_void_p), bs, flags, C.byref(loss), gptr))
     if not np.isfinite(loss.value):
         raise WustError(10, "Nonfinite objective/gradient")
+    if on_device and grad is not None:
+        grad = grad.t()
     if nargout == 1:
         return loss.value
     if nargout == 2:
@@ -171,6 +181,32 @@ def directional_curvature(state: OracleState, direction, rx_index=None, receiver
     out = C.c_double()
     check(_lib.load().wust_solver_curvature(C.c_void_p(s.handle), d.ctypes.data_as(C.c_void_p), C.byref(out)))
     return out.value
+
+
+def gauss_newton_product(state: OracleState, direction):
+    """(Re(J^H J d), d' J^H J d): the Gauss-Newton Hessian-vector product of
+    the misfit along ``direction`` with the source scales frozen (the product
+    behind directional_curvature.m's quadratic form), reusing the retained
+    factors and fields.  A CUDA tensor direction gives a CUDA tensor product."""
+    s = state.solver
+    if getattr(s, "generation", 0) != state.generation:
+        raise WustError(1, "oracle state is stale: the solver was refactored after it was produced")
+    if tuple(direction.shape) != s.shape:
+        raise WustError(1, "direction must be [ny, nx]")
+    ny, nx = s.shape
+    kappa = C.c_double()
+    lib = _lib.load()
+    if isinstance(direction, torch.Tensor) and direction.is_cuda:
+        d = direction.detach().to(torch.float64).t().contiguous()
+        out = torch.empty((nx, ny), dtype=torch.float64, device="cuda")
+        check(lib.wust_solver_gauss_newton_product(C.c_void_p(s.handle), C.c_void_p(d.data_ptr()),
+                                                   C.c_void_p(out.data_ptr()), C.byref(kappa)))
+        return out.t(), kappa.value
+    d = np.asfortranarray(np.asarray(direction, np.float64))
+    out = np.zeros((ny, nx), order="F")
+    check(lib.wust_solver_gauss_newton_product(C.c_void_p(s.handle), d.ctypes.data_as(C.c_void_p),
+                                               out.ctypes.data_as(C.c_void_p), C.byref(kappa)))
+    return out, kappa.value
 
 
 def gradient_device(c: torch.Tensor, obs: Observations, fi: int, cfg: dict, solver: HelmholtzSolver,

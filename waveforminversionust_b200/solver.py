@@ -51,6 +51,18 @@ def _fortran_device(a, dtype: torch.dtype) -> torch.Tensor:
     return t.permute(2, 1, 0).contiguous()
 
 
+def _medium_pointer(vel):
+    """A [ny, nx] medium as a column-major float64 buffer the library reads:
+    CUDA tensors stay on the device, anything else becomes a host array.
+    Returns (pointer, owner to keep alive during the call)."""
+    if isinstance(vel, torch.Tensor) and vel.is_cuda:
+        t = vel.detach().to(torch.float64).t().contiguous()       # memory [x][y] == column-major [y, x]
+        return C.c_void_p(t.data_ptr()), t
+    a = np.asfortranarray(np.asarray(vel.detach().cpu().numpy() if isinstance(vel, torch.Tensor) else vel,
+                                     dtype=np.float64))
+    return a.ctypes.data_as(C.c_void_p), a
+
+
 def _grid_vector(v) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(v, dtype=np.float64).ravel())
 
@@ -79,8 +91,7 @@ class HelmholtzSolver:
         self._x = _grid_vector(x)
         self._y = _grid_vector(y)
         ny, nx = self._y.size, self._x.size
-        vel_np = np.asarray(vel.detach().cpu().numpy() if isinstance(vel, torch.Tensor) else vel, dtype=np.float64)
-        if vel_np.shape != (ny, nx) or min(vel_np.shape) < 3:
+        if tuple(vel.shape) != (ny, nx) or min(ny, nx) < 3:
             raise WustError(1, "Expected a positive finite [ny,nx] medium")
         self.shape = (ny, nx)
         disp = options.get("dispersion") or None
@@ -118,12 +129,11 @@ class HelmholtzSolver:
         self.max_sources = opts.max_sources
         self._stream = stream or torch.cuda.current_stream()
         handle = C.c_void_p()
-        vel_c = np.asfortranarray(vel_np)
+        vel_p, self._vel_keep = _medium_pointer(vel)
         att_c = None if atten is None else np.asfortranarray(np.asarray(atten, dtype=np.float64))
         if att_c is not None and not np.any(att_c):
             att_c = None
-        self._vel_keep = vel_c
-        check(self._lib.wust_solver_create(C.byref(handle), C.byref(opts), vel_c.ctypes.data_as(C.c_void_p),
+        check(self._lib.wust_solver_create(C.byref(handle), C.byref(opts), vel_p,
                                            None if att_c is None else att_c.ctypes.data_as(C.c_void_p),
                                            C.c_void_p(self._stream.cuda_stream)))
         self._h = handle
@@ -142,16 +152,18 @@ class HelmholtzSolver:
             pass
 
     def refactor(self, vel, f=None, atten=None):
-        """Re-assemble and re-factorize for a new medium/frequency (same grid)."""
-        vel_c = np.asfortranarray(np.asarray(vel.detach().cpu().numpy() if isinstance(vel, torch.Tensor) else vel,
-                                             dtype=np.float64))
-        if vel_c.shape != self.shape:
+        """Re-assemble and re-factorize for a new medium/frequency (same grid).
+        A CUDA tensor medium stays on the device (no host copy)."""
+        if tuple(vel.shape) != self.shape:
             raise WustError(1, "Expected a positive finite [ny,nx] medium")
+        vel_p, keep = _medium_pointer(vel)
         att_c = None if atten is None else np.asfortranarray(np.asarray(atten, dtype=np.float64))
         f = self.frequency_hz if f is None else float(f)
-        check(self._lib.wust_solver_refactor(self._h, vel_c.ctypes.data_as(C.c_void_p),
+        check(self._lib.wust_solver_refactor(self._h, vel_p,
                                              None if att_c is None else att_c.ctypes.data_as(C.c_void_p),
                                              C.c_double(f)))
+        if isinstance(keep, torch.Tensor):
+            keep.record_stream(self._stream)      # the library copies it on the solver stream
         self._opts.frequency_hz = f
         self._read_meta()
 
