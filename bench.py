@@ -339,7 +339,8 @@ def run_precision(args, torch):
     def rel(a, b):
         return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
 
-    profiles = [("c64", "default"), ("c64-refined", "default"), ("tf32-refined", "default"), ("tf32-refined", "same")]
+    profiles = [("c64", "default"), ("c64-refined", "default"), ("tf32-refined", "default"), ("tf32-refined", "same"),
+                ("bf16-refined", "default")]
     finals = {}
     for prec, corr in profiles:
         rows = []
@@ -690,7 +691,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="tf32-refined")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variants", default="c64,c64-refined", help="extra precision profiles timed beside the headline")
+    ap.add_argument("--variants", default="c64,c64-refined,bf16-refined",
+                    help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
     ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision", "autograd", "batch"],
                     help="solve: factor once, then time forward solves of all transmitters (kernel profiling); "
@@ -927,7 +929,8 @@ def main():
     line = dict(metric="gradients_per_second", value=head["value"], unit="gradients/s", n_gpus=world,
                 steps=args.steps, warmup=args.warmup, ms_per_step=head["ms_per_step"], higher_is_better=True,
                 scaling="weak", vs_baseline=None,
-                dtype={"c64": "c64", "c64-refined": "c64+c128-refine"}.get(args.precision, "tf32+c128-refine"),
+                dtype={"c64": "c64", "c64-refined": "c64+c128-refine",
+                       "bf16-refined": "bf16+tf32-factor+c128-refine"}.get(args.precision, "tf32+c128-refine"),
                 data="synthetic",
                 config=dict(workload=WORKLOADS[WORKLOAD]["text"], medium=HEADLINE_MEDIUM,
                             global_batch=N_TX * world, precision=args.precision, parallelism=f"replicas{world}",

@@ -57,7 +57,8 @@ enum wust_status {
 enum wust_precision {
     WUST_PRECISION_C64 = 0,          /* plain complex-single block LU: the reference algorithm */
     WUST_PRECISION_C64_REFINED = 1,  /* c64 block LU + FP64-residual iterative refinement */
-    WUST_PRECISION_BF16_REFINED = 2, /* BF16 tensor-core Schur/solve GEMMs + FP64 refinement */
+    WUST_PRECISION_BF16_REFINED = 2, /* BF16 tensor-core sweep GEMMs for every solve (TF32 Newton-Schulz
+                                        Schur inverses) + FP64 refinement; needs the column-chunked sweeps */
     WUST_PRECISION_TF32_REFINED = 3  /* TF32 tensor-core Schur/solve GEMMs + FP64 refinement */
 };
 

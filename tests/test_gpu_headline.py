@@ -30,7 +30,7 @@ FREQ = 1.2e6
 SAMPLE = [0, 37, 73, 110, 146, 183, 219, 255]
 GRAD_TX = list(range(0, 256, 16))
 MODELS = ("homogeneous", "textured")
-PROFILES = ("tf32-refined", "c64-refined")
+PROFILES = ("tf32-refined", "c64-refined", "bf16-refined")
 
 
 def rel(a, b):

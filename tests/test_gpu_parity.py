@@ -110,7 +110,7 @@ def test_solve_matches_sparse_lu(small):
     s.close()
 
 
-@pytest.mark.parametrize("precision", ["c64-refined", "tf32-refined"])
+@pytest.mark.parametrize("precision", ["c64-refined", "tf32-refined", "bf16-refined"])
 def test_refined_solve_reaches_fp64_accuracy(small, precision):
     p, ref = small
     from oracle import helmholtz_fp64 as o
@@ -399,7 +399,8 @@ def test_config1_gradient_parity():
     # Refined profiles stop at an estimated forward error of 1e-5 (the pressure
     # tolerance); the TF32 sweeps contract less per correction than the
     # complex-single ones, so their misfit is held to that 1e-5 bound.
-    for precision, tl, tg in (("c64", 1e-3, 1e-2), ("c64-refined", 1e-6, 1e-4), ("tf32-refined", 1e-5, 1e-4)):
+    for precision, tl, tg in (("c64", 1e-3, 1e-2), ("c64-refined", 1e-6, 1e-4), ("tf32-refined", 1e-5, 1e-4),
+                              ("bf16-refined", 1e-5, 1e-4)):
         loss, grad = wust_oracle(p.c_init, obs, 0, default_config(pml_m=p.pml_m, precision=precision))
         assert abs(loss - loss_ref) / loss_ref < tl, precision
         assert rel(grad, grad_ref) < tg, precision

@@ -203,7 +203,7 @@ def test_autograd_forward_only_and_gauss_newton_products(ref_fixture):
     n0 = solver.sweep_times()[1]
     l2 = misfit(s1, obs, 0, cfg)
     pairs_gradient = solver.sweep_times()[1] - n0
-    assert float(l0) == float(l1) and abs(float(l2) - float(l1)) <= 1e-12 * float(l1)
+    assert float(l0) == float(l1) and abs(float(l2.detach()) - float(l1)) <= 1e-12 * float(l1)
     assert 0 < pairs_forward < pairs_gradient, (pairs_forward, pairs_gradient)
     (g,) = torch.autograd.grad(l2, s1, create_graph=True)
     assert g.is_cuda

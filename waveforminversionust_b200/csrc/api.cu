@@ -159,9 +159,11 @@ struct wust_solver {
     float *ck_z = nullptr, *ck_sb = nullptr;
     float2 *ck_edges = nullptr;
     unsigned *ck_sync = nullptr;
-    // BF16 operands of the correction sweeps (TF32 profile, chunked sweeps)
+    // BF16 operands of the correction sweeps (TF32 profile, chunked sweeps),
+    // or of every sweep (BF16 profile)
     int correction_precision = WUST_CORRECTION_DEFAULT;
     bool bf16_corrections = false;
+    bool bf16_all = false;
     uint8_t *tc_afwd16 = nullptr, *tc_aadj16 = nullptr, *ck_lpack16 = nullptr;
     TcChunkBuffers chunk_buffers() const {
         return TcChunkBuffers{ck_lpack, ck_b, ck_lpack16, ck_z, ck_sb, ck_edges, ck_sync, tc_err};
@@ -241,6 +243,13 @@ static std::vector<double> linspace(double a, double b, int n) {
     return v;
 }
 
+// The tensor-core profiles: Newton-Schulz TF32 Schur inverses and tcgen05
+// sweeps (TF32 operands, BF16 for corrections by default; the BF16 profile
+// puts every sweep on BF16 operands).
+static bool tensor_profile(const wust_solver *s) {
+    return s->precision == WUST_PRECISION_TF32_REFINED || s->precision == WUST_PRECISION_BF16_REFINED;
+}
+
 static void assemble_and_factor(wust_solver *s, const double *vel_in, const double *atten_in) {
     cudaStream_t st = s->st;
     const size_t N = s->plane();
@@ -291,7 +300,7 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
         if (astat == 2) fail(WUST_ERR_INVALID_INPUT, "k-Wave local dispersion target is evanescent");
         if (astat == 3) fail(WUST_ERR_NUMERICAL_FAILURE, "LDR-9 produced invalid wavenumber or derivative");
     };
-    if (s->precision == WUST_PRECISION_TF32_REFINED && s->ns_scratch) {
+    if (tensor_profile(s) && s->ns_scratch) {
         // the iteration needs a valid operator: check the assembly first
         int astat0 = 0;
         WUST_CUDA(cudaMemcpyAsync(&astat0, s->status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -303,7 +312,7 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
     } else {
         factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
     }
-    if (s->precision == WUST_PRECISION_TF32_REFINED) {
+    if (tensor_profile(s)) {
         if (s->bf16_corrections && s->use_chunks && s->ck_geom.kc == s->tc_geom.kc && s->ck_geom.mt == s->tc_geom.mt)
             tc_pack_invT_both(s->invT, s->ny, s->nx, s->ck_geom, s->tc_afwd, s->tc_aadj, s->tc_afwd16, s->tc_aadj16, st);
         else {
@@ -354,8 +363,8 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
 // complex single, or tcgen05 TF32 GEMMs on the packed invT operands.
 static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out, bool correction = false) {
     WUST_CUDA(cudaEventRecord(s->sw_ev[0], s->st));
-    if (s->precision == WUST_PRECISION_TF32_REFINED) {
-        const bool bf16 = correction && s->bf16_corrections;
+    if (tensor_profile(s)) {
+        const bool bf16 = s->bf16_all || (correction && s->bf16_corrections);
         if (s->use_chunks)
             tc_chunk_solve(s->coefs64(), bf16 ? s->tc_afwd16 : s->tc_afwd, bf16 ? s->tc_aadj16 : s->tc_aadj, s->ck_geom,
                            s->chunk_buffers(), src, S, adjoint, out, bf16, s->st);
@@ -577,8 +586,6 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         if (!(o->frequency_hz > 0) || !(o->pml_m > 0) || !std::isfinite(o->pml_strength))
             fail(WUST_ERR_INVALID_INPUT, "frequency, pml_m and pml_strength must be positive and finite");
         if (o->precision < 0 || o->precision > 3) fail(WUST_ERR_INVALID_INPUT, "unknown precision profile");
-        if (o->precision == WUST_PRECISION_BF16_REFINED)
-            fail(WUST_ERR_INVALID_INPUT, "the BF16 profile is not available in this build; use TF32");
         if (o->dispersion && !(o->time_step_s > 0 && o->reference_speed_mps > 0))
             fail(WUST_ERR_INVALID_INPUT, "LDR9 requires explicit simulation dispersion facts");
         s = new wust_solver();
@@ -655,7 +662,9 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
             s->dnorm2 = dalloc<double>(s->smax);
             s->xnorm2 = dalloc<double>(s->smax);
         }
-        if (s->precision == WUST_PRECISION_TF32_REFINED) {
+        if (s->precision == WUST_PRECISION_BF16_REFINED && s->sweep_method != WUST_SWEEP_DEFAULT)
+            fail(WUST_ERR_INVALID_INPUT, "the BF16 profile runs on the column-chunked sweeps (sweep_method default)");
+        if (tensor_profile(s)) {
             s->tc_geom = tc_sweep_geom(ny, s->smax, tc_sweep_max_ctas());
             s->tc_afwd = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
             s->tc_aadj = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
@@ -681,13 +690,19 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
                 WUST_CUDA(cudaMemset(s->ck_sb, 0, s->ck_geom.state_bytes));
                 s->ck_sync = dalloc<unsigned>(s->ck_geom.sync_words);
                 s->ck_edges = dalloc<float2>(s->ck_geom.edge_bytes / sizeof(float2));
-                s->bf16_corrections = s->correction_precision == WUST_CORRECTION_DEFAULT;
+                // BF16 profile: every sweep on BF16 operands (correction_precision
+                // SAME keeps the corrections on the profile's operands: BF16 too)
+                s->bf16_all = s->precision == WUST_PRECISION_BF16_REFINED;
+                s->bf16_corrections = s->bf16_all || s->correction_precision == WUST_CORRECTION_DEFAULT;
                 if (s->bf16_corrections) {
                     s->tc_afwd16 = dalloc<uint8_t>(s->ck_geom.page_bytes16 * nx);
                     s->tc_aadj16 = dalloc<uint8_t>(s->ck_geom.page_bytes16 * nx);
                     if (s->ck_geom.lpack16_bytes) s->ck_lpack16 = dalloc<uint8_t>(s->ck_geom.lpack16_bytes);
                 }
             }
+            if (s->precision == WUST_PRECISION_BF16_REFINED && !s->use_chunks)
+                fail(WUST_ERR_INVALID_INPUT, "the BF16 profile runs on the column-chunked sweeps; the grid has too "
+                                             "few columns for two chunks (use tf32-refined)");
         }
         assemble_and_factor(s, vel, atten);
         *out = s;
@@ -1134,7 +1149,7 @@ int wust_solver_sweep_times(const wust_solver *s, double *total_ms, long long *c
 int wust_solver_factor_stats(const wust_solver *s, long long out[4]) {
     return guarded([&] {
         if (!s || !out) fail(WUST_ERR_INVALID_INPUT, "null solver or output");
-        if (s->precision == WUST_PRECISION_TF32_REFINED && s->ns_scratch) {
+        if (tensor_profile(s) && s->ns_scratch) {
             for (int i = 0; i < 4; ++i) out[i] = s->ns_stats[i];
         } else {
             out[0] = out[1] = out[2] = 0;
