@@ -13,7 +13,7 @@
 // R_k (||R_k||_F / sqrt(n), summed in a fixed order so every CTA decides
 // alike):
 //     r_k <= kAccept                      accept X_k
-//     r_k <= kLastUpdate, or stalled      one more update, accept
+//     r_k <= kLastUpdate(First), stalled  one more update, accept
 //     diverging / not contracting         give the column back (Gauss-Jordan)
 // Columns where X_{j-1} is no start (the Dirichlet columns, the first
 // columns after them) go to the Gauss-Jordan kernel; the host driver
@@ -56,12 +56,15 @@ static_assert(kNsSmem <= 232448, "shared memory of one CTA");
 constexpr int kTmemCols = 128;
 
 constexpr float kAccept = 2e-4f;        // residual small enough: keep X_k
-// One more update, then accept: r^2 <= 9e-4, within three times the TF32
-// floor (~3.5e-4).  Measured at 552^2, 256 sources, 1.2 MHz on a textured
-// medium: 1e-2 -> 3.7 GEMMs per page, 51 ms; 3e-2 -> 2.8, 42.7 ms, with the
-// same two refinement corrections per solve and pressure / gradient within
-// 3.5e-6 / 2.0e-6 of the FP64 sparse LU; 5e-2 and above add a correction.
-constexpr float kLastUpdate = 3e-2f;
+// One more update, then accept: from the page's first residual (the
+// previous page's inverse as the start) when r_0 <= kLastUpdateFirst (the
+// accepted page then has r ~ 4e-4, at the TF32 floor of ~3.5e-4), from a
+// later residual when r_k <= kLastUpdate.  Measured at 552^2, 256 sources,
+// 1.2 MHz: (3e-2, 1e-2) saves 8 ms of factorization on a half-textured
+// medium but the fully textured one then needs a third refinement
+// correction; (2e-2, 1e-2) keeps two corrections on both and saves 2.3 ms.
+constexpr float kLastUpdateFirst = 2e-2f;
+constexpr float kLastUpdate = 1e-2f;
 constexpr float kFirstFail = 0.8f;      // X_{j-1} is no start for this column
 constexpr float kStallAccept = 0.05f;   // stalled at this level: finish with one update
 
@@ -567,7 +570,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 int dec;                          // 0 accept, 1 last update, 2 update, 3 fail
                 if (!(r_k == r_k) || r_k > 1e30f) dec = 3;
                 else if (r_k <= kAccept) dec = 0;
-                else if (r_k <= kLastUpdate) dec = 1;
+                else if (r_k <= (k == 0 ? kLastUpdateFirst : kLastUpdate)) dec = 1;
                 else if (k > 0 && r_k >= r_prev) dec = 3;
                 else if (k > 0 && r_k > 0.3f * r_prev && r_k < kStallAccept) dec = 1;
                 else if ((k == 0 && r_k > kFirstFail) || k >= p.max_iter) dec = 3;
