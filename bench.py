@@ -479,72 +479,53 @@ def batch_problems(seed: int = 0, count: int = 24):
     return probs
 
 
-class _GradientRun:
-    """One problem's gradient through the C ABI with device-resident inputs
-    (refactor + wust_solver_oracle with the gradient), on a given stream."""
-
-    def __init__(self, p, stream, torch, precision):
-        from waveforminversionust_b200 import _lib
-        from waveforminversionust_b200.solver import HelmholtzSolver
-        self.lib, self.check, self.need = _lib.load(), _lib.check, _lib.NEED_GRADIENT
-        ny, nx = p.shape
-        self.n_tx, self.n_rx, self.f = p.tx_index.size, p.rx_index.size, float(p.frequencies_hz[0])
-        self.solver = HelmholtzSolver(p.x_m, p.y_m, p.c_init, None, self.f, -1, 10.0, p.pml_m,
-                                      dict(backend="gpu", stencil_bounds=(1400, 1700)), precision=precision,
-                                      max_sources=self.n_tx, stream=stream)
-        rng = np.random.default_rng(ny * 1000 + self.n_tx)
-        Y = (rng.standard_normal((self.n_tx, self.n_rx)) + 1j * rng.standard_normal((self.n_tx, self.n_rx))) * 1e-3
-        self.c = torch.as_tensor(np.asfortranarray(p.c_init).T.copy(), device="cuda")
-        self.tx = torch.as_tensor(p.tx_index.astype(np.int32), device="cuda")
-        self.rx = torch.as_tensor(p.rx_index.astype(np.int32), device="cuda")
-        self.Y = torch.as_tensor(np.asfortranarray(Y).T.astype(np.complex64).copy(), device="cuda")
-        self.m = torch.ones((self.n_rx, self.n_tx), dtype=torch.uint8, device="cuda")
-        self.g = torch.empty((nx, ny), dtype=torch.float64, device="cuda")
-        self.loss = C.c_double()
-
-    def run(self):
-        h = C.c_void_p(self.solver.handle)
-        self.check(self.lib.wust_solver_refactor(h, C.c_void_p(self.c.data_ptr()), None, C.c_double(self.f)))
-        self.check(self.lib.wust_solver_oracle(h, C.c_void_p(self.tx.data_ptr()), self.n_tx,
-                                               C.c_void_p(self.rx.data_ptr()), self.n_rx, C.c_void_p(self.Y.data_ptr()),
-                                               C.c_void_p(self.m.data_ptr()), self.n_tx, self.need,
-                                               C.byref(self.loss), C.c_void_p(self.g.data_ptr())))
-
-    def close(self):
-        self.solver.close()
-
-
 def run_batch(args, torch):
     """Config 5: 24 independent inversions of uneven size, one gradient each
-    (tf32-refined), run one after another: each gradient is timed with CUDA
-    events on its solver's stream after a warm-up gradient, the aggregate is
-    24 / the sum of the gradient times, and the per-problem latency is listed.
-    The problems are not run concurrently: the factorization and the sweeps
-    are persistent kernels whose grid barriers need all their CTAs resident,
-    which two such launches sharing the GPU would not guarantee.  Solvers are
-    built outside the timed regions, one at a time."""
+    (tf32-refined).  First every problem alone on the whole GPU, one after
+    another (the reference's way: one problem at a time); then the
+    autotuner's plan: problems that gain from sharing run concurrently on
+    SM partitions (one stream and host thread per partition, cooperative
+    kernels capped to the partition), the others alone first.  Both makespans
+    are device time (events) over all 24 gradients after a warm-up gradient
+    of every problem; solvers are built outside the timed regions.  The
+    autotuner's measurements are timed separately."""
+    from waveforminversionust_b200.batch import Autotuner, BatchProblem, Plan, run_batch as run_plan
     probs = batch_problems()
-    precision = args.precision
-    stream = torch.cuda.Stream()
-    seq = []
-    for p in probs:
-        r = _GradientRun(p, stream, torch, precision)
-        r.run()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        r.run()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        seq.append(dict(grid=p.shape[0], n_tx=int(p.tx_index.size), n_rx=int(p.rx_index.size),
-                        f_mhz=round(float(p.frequencies_hz[0]) / 1e6, 3), ms=round(e0.elapsed_time(e1), 3)))
-        r.close()
-    t_seq = sum(x["ms"] for x in seq)
-    print(json.dumps(dict(mode="batch", precision=precision, problems=len(probs),
+    problems = []
+    for k, p in enumerate(probs):
+        rng = np.random.default_rng(1000 + k)
+        n_tx, n_rx = p.tx_index.size, p.rx_index.size
+        Y = (rng.standard_normal((n_tx, n_rx)) + 1j * rng.standard_normal((n_tx, n_rx))) * 1e-3
+        problems.append(BatchProblem(p.x_m, p.y_m, p.c_init, float(p.frequencies_hz[0]), p.pml_m, p.tx_index,
+                                     p.rx_index, Y, np.ones((n_tx, n_rx), bool), precision=args.precision,
+                                     name=p.name))
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    seq_plan = Plan(parts=1, cap=n_sm, exclusive=list(range(len(problems))), groups=[[]])
+    seq = run_plan(problems, seq_plan)
+    t0 = time.perf_counter()
+    tuner = Autotuner(parts=(2, 3, 4), repeats=2)
+    pl = tuner.tune(problems, n_sm=n_sm)
+    tune_s = time.perf_counter() - t0
+    par = run_plan(problems, pl)
+    rows = []
+    for i, p in enumerate(problems):
+        rows.append(dict(grid=p.shape[0], n_tx=int(p.tx_index.size), n_rx=int(p.rx_index.size),
+                         f_mhz=round(p.frequency_hz / 1e6, 3), alone_ms=round(seq["per_problem_ms"][i], 3),
+                         planned_ms=round(par["per_problem_ms"][i], 3),
+                         setting="whole GPU" if i in pl.exclusive else f"partition of {pl.cap} SMs",
+                         chunks=pl.chunks.get(i, 0)))
+    print(json.dumps(dict(mode="batch", precision=args.precision, problems=len(problems),
                           workload="config5: 24 independent inversions, interiors {128..512}^2 + 16-20 PML, "
                                    "dx 0.25-0.4 mm, 16-256 TX, one frequency each in 0.3-1.2 MHz",
-                          value=len(probs) / (t_seq * 1e-3), unit="gradients/s", total_ms=t_seq,
-                          per_problem=seq)), flush=True)
+                          unit="gradients/s", sequential=dict(value=seq["gradients_per_second"],
+                                                              makespan_ms=seq["makespan_s"] * 1e3),
+                          planned=dict(value=par["gradients_per_second"], makespan_ms=par["makespan_s"] * 1e3,
+                                       exclusive_ms=par["exclusive_s"] * 1e3, concurrent_ms=par["concurrent_s"] * 1e3,
+                                       predicted_ms=pl.predicted_s * 1e3),
+                          speedup=seq["makespan_s"] / par["makespan_s"],
+                          plan=dict(parts=pl.parts, cap=pl.cap, exclusive=pl.exclusive, groups=pl.groups),
+                          autotuner=dict(seconds=round(tune_s, 1), measurements=tuner.measured),
+                          per_problem=rows)), flush=True)
 
 
 def run_dtft(args, torch):

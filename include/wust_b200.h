@@ -146,6 +146,10 @@ typedef struct {
     int factor_method;             /* WUST_FACTOR_*: how the Schur pages are inverted */
     int sweep_method;              /* WUST_SWEEP_*: how the TF32 profile runs its sweeps */
     int correction_precision;      /* WUST_CORRECTION_*: operands of the refinement's correction sweeps */
+    int max_ctas;                  /* > 0: cap on the CTAs (one per SM) of the solver's cooperative kernels, so that
+                                      solvers on different streams can share the GPU; 0: the whole GPU */
+    int chunk_count;               /* > 0: column chunks of the chunked sweeps (clamped to what fits); 0: about
+                                      sqrt(2 (Nx - 1)) */
 } wust_solver_options;
 
 /* Schur-page inversion (no counterpart in the reference, which always uses

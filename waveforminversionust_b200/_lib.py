@@ -55,6 +55,7 @@ class SolverOptions(C.Structure):
         ("dispersion", C.c_int), ("time_step_s", C.c_double), ("reference_speed_mps", C.c_double),
         ("precision", C.c_int), ("refine_max_iters", C.c_int), ("refine_tol", C.c_double),
         ("max_sources", C.c_int), ("factor_method", C.c_int), ("sweep_method", C.c_int), ("correction_precision", C.c_int),
+        ("max_ctas", C.c_int), ("chunk_count", C.c_int),
     ]
 
 

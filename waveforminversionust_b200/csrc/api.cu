@@ -96,6 +96,8 @@ struct wust_solver {
     int ny = 0, nx = 0, smax = 0, precision = 0, refine_max = 8;
     double refine_tol = 1e-5;
     int factor_method = WUST_FACTOR_DEFAULT;
+    int max_ctas = 0;      // > 0: cooperative grids capped (a solver confined to part of the GPU)
+    int chunk_count = 0;   // > 0: column chunks of the chunked sweeps
     int sweep_method = WUST_SWEEP_DEFAULT;
     // NCG update on the device: real 2-D FFT plans of the grid, half spectrum,
     // block partials of the reductions (created on first use)
@@ -308,9 +310,9 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
         check_assembly(astat0);
         for (long long &v : s->ns_stats) v = 0;
         ns_factor(s->coefs64(), s->invT, s->ns_g, s->ns_scratch, s->fscratch, s->fscratch_bytes, st, s->ns_stats,
-                  &s->ns_head);
+                  &s->ns_head, s->max_ctas);
     } else {
-        factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat);
+        factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat, 0, -1, s->max_ctas);
     }
     if (tensor_profile(s)) {
         if (s->bf16_corrections && s->use_chunks && s->ck_geom.kc == s->tc_geom.kc && s->ck_geom.mt == s->tc_geom.mt)
@@ -600,6 +602,9 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         if (o->correction_precision < WUST_CORRECTION_DEFAULT || o->correction_precision > WUST_CORRECTION_SAME)
             fail(WUST_ERR_INVALID_INPUT, "unknown correction_precision %d", o->correction_precision);
         s->correction_precision = o->correction_precision;
+        if (o->max_ctas < 0 || o->chunk_count < 0) fail(WUST_ERR_INVALID_INPUT, "max_ctas and chunk_count must be >= 0");
+        s->max_ctas = o->max_ctas;
+        s->chunk_count = o->chunk_count;
         s->precision = o->precision;
         s->refine_max = o->refine_max_iters > 0 ? o->refine_max_iters : 8;
         s->refine_tol = o->refine_tol > 0 ? o->refine_tol : 1e-5;
@@ -665,20 +670,21 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
         if (s->precision == WUST_PRECISION_BF16_REFINED && s->sweep_method != WUST_SWEEP_DEFAULT)
             fail(WUST_ERR_INVALID_INPUT, "the BF16 profile runs on the column-chunked sweeps (sweep_method default)");
         if (tensor_profile(s)) {
-            s->tc_geom = tc_sweep_geom(ny, s->smax, tc_sweep_max_ctas());
+            auto capped = [&](int device_max) { return s->max_ctas > 0 ? std::min(device_max, s->max_ctas) : device_max; };
+            s->tc_geom = tc_sweep_geom(ny, s->smax, capped(tc_sweep_max_ctas()));
             s->tc_afwd = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
             s->tc_aadj = dalloc<uint8_t>(s->tc_geom.page_bytes * nx);
             s->tc_b = dalloc<uint8_t>(s->tc_geom.b_bytes);
             s->tc_part = dalloc<float>(s->tc_geom.part_bytes / sizeof(float));
             s->tc_sync = dalloc<unsigned>(s->tc_geom.sync_words);
             if (s->factor_method == WUST_FACTOR_DEFAULT) {
-                s->ns_g = ns_geom(ny, ns_max_ctas());
+                s->ns_g = ns_geom(ny, capped(ns_max_ctas()));
                 if (s->ns_g.ks > 0) WUST_CUDA(cudaMalloc(&s->ns_scratch, s->ns_g.scratch_bytes));
             }
             s->tc_err = dalloc<int>(4);
             WUST_CUDA(cudaMemset(s->tc_err, 0, 4 * sizeof(int)));
             if (s->sweep_method == WUST_SWEEP_DEFAULT) {
-                s->ck_geom = tc_chunk_geom(ny, nx, tc_chunk_max_ctas());
+                s->ck_geom = tc_chunk_geom(ny, nx, capped(tc_chunk_max_ctas()), s->chunk_count);
                 s->use_chunks = s->ck_geom.C >= 2;   // one chunk: the sequential kernel is faster
             }
             if (s->use_chunks) {

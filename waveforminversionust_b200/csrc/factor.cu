@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(GT, 1) factor_kernel(FactorParams p) {
 size_t factor_scratch_bytes(int ny) { return factor_scratch_bytes_for(ny); }
 
 void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t scratch_bytes,
-                   cudaStream_t stream, double timeout_s, int *host_status, int j0, int j1) {
+                   cudaStream_t stream, double timeout_s, int *host_status, int j0, int j1, int max_ctas) {
     const int ny = co.ny;
     const int n = ny - 2;
     const int np_ = (int)factor_pad(ny);
@@ -392,6 +392,7 @@ void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t 
     if (per_sm < 1) fail(WUST_ERR_CUDA, "factor kernel cannot be resident");
     const int nt = np_ / G;
     int grid = sms;                          // one CTA per SM
+    if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
     if (grid > nt * nt) grid = nt * nt;
     void *args[] = {&p};
     WUST_CUDA(cudaLaunchCooperativeKernel((void *)factor_kernel, dim3(grid), dim3(GT), args, kFactorSmemBytes, stream));

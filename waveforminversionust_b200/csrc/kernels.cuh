@@ -15,8 +15,10 @@ size_t factor_scratch_bytes(int ny);
 // host_status (nullable, int[3]): {1+bad page, pivot, barrier timeout site};
 // when non-null the call synchronizes the stream.  Pages [j0, j1) are
 // factored (j1 < 0: through the last page); page j0 - 1 must already be in invT.
+// max_ctas > 0 caps the cooperative grid (a solver confined to part of the GPU).
 void factor_launch(const Coefs<float2> &co, float2 *invT, void *scratch, size_t scratch_bytes,
-                   cudaStream_t stream, double timeout_s, int *host_status, int j0 = 0, int j1 = -1);
+                   cudaStream_t stream, double timeout_s, int *host_status, int j0 = 0, int j1 = -1,
+                   int max_ctas = 0);
 int barrier_selftest(double timeout_s, int *site_out);
 
 // ---- sweep.cu --------------------------------------------------------------
@@ -72,7 +74,8 @@ struct TcChunkBuffers {
     unsigned *sync;
     int *err;
 };
-TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas);
+// chunks > 0 asks for that many column chunks (clamped to what fits).
+TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas, int chunks = 0);
 int tc_chunk_max_ctas();
 size_t tc_chunk_state_floats(int ny);
 // Composed propagators of the chunks of all four substitutions (after tc_pack_invT).
@@ -126,7 +129,7 @@ int ns_max_ctas();
 // (at least 3); the pages before it go to one Gauss-Jordan launch.  Updated
 // from this factorization for the next one of the same solver.
 void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
-               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint);
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint, int max_ctas = 0);
 
 // ---- assemble.cu -----------------------------------------------------------
 struct AssemblyInput {

@@ -769,11 +769,11 @@ __global__ void identity_page_kernel(Coefs<float2> co, float2 *invT, int j, int 
 }
 
 void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
-               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint) {
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint, int max_ctas) {
     const int nx = co.nx;
     int hstat[3];
     auto gj = [&](int a, int b) {
-        factor_launch(co, invT, gj_scratch, gj_scratch_bytes, st, 10.0, hstat, a, b);
+        factor_launch(co, invT, gj_scratch, gj_scratch_bytes, st, 10.0, hstat, a, b, max_ctas);
         if (hstat[2]) fail(WUST_ERR_DEVICE_TIMEOUT, "factorization barrier timed out (site %d)", hstat[2]);
         if (hstat[0])
             fail(WUST_ERR_SINGULAR_SCHUR_BLOCK, "Schur block %d is singular (pivot %d)", hstat[0] - 1, hstat[1]);

@@ -68,7 +68,7 @@ enum CkProduce { P_STENCIL = 0, P_IDENT = 1, P_TURN = 2 };
 
 size_t tc_chunk_state_floats(int ny) { return (size_t)2 * kCkMaxN * ny; }
 
-TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas) {
+TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas, int chunks) {
     TcChunkGeom g{};
     g.n = ny - 2;
     g.mt = ceil_div(g.n, 64);
@@ -81,7 +81,7 @@ TcChunkGeom tc_chunk_geom(int ny, int nx, int max_ctas) {
     // about sqrt(2 steps) chunks balance the two passes against the boundary
     // chain; every chunk keeps at least 2 steps (the mirrored H^H backward
     // cuts then leave no chunk empty)
-    int C = (int)std::lround(std::sqrt(2.0 * steps));
+    int C = chunks > 0 ? chunks : (int)std::lround(std::sqrt(2.0 * steps));
     C = std::max(1, std::min({C, max_ctas / g.mt, steps / 2, kCkMaxChunks}));
     g.C = C;
     g.page_bytes = (size_t)g.mt * g.kc * tc::kAChunk;

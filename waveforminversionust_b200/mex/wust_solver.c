@@ -13,7 +13,8 @@
  *       ('c64' | 'c64-refined' | 'tf32-refined', default 'c64'), refine_tol
  *       (default 1e-5), refine_max_iters (8), max_sources (256),
  *       factor_method ('default' | 'gauss-jordan'), sweep_method
- *       ('default' | 'sequential'), correction_precision ('default' | 'same').
+ *       ('default' | 'sequential'), correction_precision ('default' | 'same'),
+ *       max_ctas (0: the whole GPU), chunk_count (0: automatic).
  *       h is a uint64 scalar naming the live solver.
  *   wust_solver('refactor', h, vel, atten, f)       new medium / frequency, same grid
  *   [u, virt] = wust_solver('solve', h, src, adjoint)   (HelmholtzSolver.m:174-203)
@@ -176,6 +177,8 @@ static void cmd_create(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[
     o.factor_method = choice(opts, "factor_method", defaults2, 2, WUST_FACTOR_DEFAULT);
     o.sweep_method = choice(opts, "sweep_method", sweeps, 2, WUST_SWEEP_DEFAULT);
     o.correction_precision = choice(opts, "correction_precision", corrections, 2, WUST_CORRECTION_DEFAULT);
+    o.max_ctas = (int)option_scalar(opts, "max_ctas", 0);
+    o.chunk_count = (int)option_scalar(opts, "chunk_count", 0);
     for (slot = -1, i = 0; i < MAX_SOLVERS; ++i)
         if (!live[i]) {
             slot = i;

@@ -84,14 +84,14 @@ class _SolverPool:
                tuple(map(float, cfg["stencil_bounds"])), cfg.get("precision", "c64"),
                int(min(cfg.get("source_batch_size", 256), obs.n_tx)), float(cfg.get("refine_tol", 1e-5)),
                None if not disp else (float(disp["time_step_s"]), float(disp["reference_speed_mps"])),
-               cfg.get("correction_precision", "default"))
+               cfg.get("correction_precision", "default"), int(cfg.get("max_ctas", 0)), int(cfg.get("chunk_count", 0)))
         f = float(obs.frequencies_hz[fi])
         s = self._pool.get(key)
         if s is None:
             s = HelmholtzSolver(obs.x_m, obs.y_m, c, None, f, -1, cfg["pml_strength"], cfg["pml_m"],
                                 dict(backend="gpu", stencil_bounds=cfg["stencil_bounds"], dispersion=disp),
                                 precision=cfg.get("precision", "c64"), max_sources=key[7], refine_tol=key[8],
-                                correction_precision=key[10])
+                                correction_precision=key[10], max_ctas=key[11], chunk_count=key[12])
             s.generation = 0
             self._pool[key] = s
         else:

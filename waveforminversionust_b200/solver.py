@@ -74,7 +74,7 @@ class HelmholtzSolver:
                  precision: str = "c64", refine_tol: float = 1e-5, refine_max_iters: int = 8,
                  max_sources: int | None = None, stream: torch.cuda.Stream | None = None,
                  factor_method: str = "default", sweep_method: str = "default",
-                 correction_precision: str = "default"):
+                 correction_precision: str = "default", max_ctas: int = 0, chunk_count: int = 0):
         if not isinstance(options, dict) or "backend" not in options or "stencil_bounds" not in options:
             raise WustError(1, "Explicit backend and fixed stencil_bounds are required")
         bounds = options["stencil_bounds"]
@@ -124,6 +124,8 @@ class HelmholtzSolver:
             raise WustError(1, f"correction_precision must be one of {sorted(corrections)}")
         opts.correction_precision = corrections[correction_precision]
         opts.max_sources = int(max_sources or 256)
+        opts.max_ctas = int(max_ctas)
+        opts.chunk_count = int(chunk_count)
         self._opts = opts
         self.precision = precision
         self.max_sources = opts.max_sources
