@@ -48,7 +48,7 @@ def test_concurrent_partitions_match_whole_gpu_and_fp64_oracle():
     for i, (loss_ref, grad_ref) in enumerate(refs):
         g_alone, g_shared = alone["gradients"][i], shared["gradients"][i]
         assert rel(g_shared, g_alone) < 1e-5, i
-        assert abs(shared["losses"][i] - loss_ref) / loss_ref < 1e-5, i
+        assert abs(shared["losses"][i] - loss_ref) / loss_ref < 3e-5, i
         assert rel(g_shared, grad_ref) < 1e-4, i
     # the autotuner's own plan runs and gives the same gradients
     pl = Autotuner(parts=(2, 4), repeats=1).tune(problems, n_sm=n_sm)

@@ -362,11 +362,12 @@ static void ensure_obs(wust_solver *s, int n_tx, int n_rx) {
 }
 
 // One sweep pair (forward+backward) with the profile's arithmetic: CUDA-core
-// complex single, or tcgen05 TF32 GEMMs on the packed invT operands.
-static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out, bool correction = false) {
+// complex single, or tcgen05 GEMMs on the packed invT operands (TF32, or BF16
+// when bf16 is set and the solver holds BF16 operands).
+static void run_sweep(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out, bool bf16 = false) {
     WUST_CUDA(cudaEventRecord(s->sw_ev[0], s->st));
     if (tensor_profile(s)) {
-        const bool bf16 = s->bf16_all || (correction && s->bf16_corrections);
+        bf16 = bf16 && s->tc_afwd16 != nullptr;
         if (s->use_chunks)
             tc_chunk_solve(s->coefs64(), bf16 ? s->tc_afwd16 : s->tc_afwd, bf16 ? s->tc_aadj16 : s->tc_aadj, s->ck_geom,
                            s->chunk_buffers(), src, S, adjoint, out, bf16, s->st);
@@ -409,12 +410,18 @@ static void check_tc_err(wust_solver *s) {
 // the unrefined c64 solution while its error is not).
 static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
     cudaStream_t st = s->st;
-    run_sweep(s, src, S, adjoint, out);
+    run_sweep(s, src, S, adjoint, out, s->bf16_all);
     s->last_refine_iters = 0;
     s->last_residual = -1;
     s->last_error_est = -1;
     if (s->precision == WUST_PRECISION_C64) return;
     std::vector<double> rn(S), rn_prev(S), bn(S), dn(S), xn(S);
+    // BF16 corrections (half the operand bytes) as long as they contract the
+    // residual at least kBf16Contraction-fold per correction; a weaker step
+    // (poorly conditioned operators, long chunks whose BF16 propagators lose
+    // accuracy) turns the rest of this solve's corrections to TF32 operands
+    constexpr double kBf16Contraction = 0.2;
+    bool bf16_corr = s->bf16_all || s->bf16_corrections;
     SrcView dense{};
     dense.mode = SRC_DENSE;
     dense.dense = s->r32;
@@ -430,7 +437,7 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
             fail(WUST_ERR_NOT_CONVERGED, "refinement did not reach %.1e after %d correction solves (estimate %.3e)",
                  s->refine_tol, s->refine_max, s->last_error_est);
         rn_prev = rn;
-        run_sweep(s, dense, S, adjoint, s->d32, true);
+        run_sweep(s, dense, S, adjoint, s->d32, bf16_corr);
         if (!xa) {
             refine_step_launch(rw, src, s->d32, out, nullptr, S, adjoint, xb, nullptr, s->r32, s->rnorm2, s->dnorm2,
                                s->xnorm2, st);
@@ -447,19 +454,21 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
         WUST_CUDA(cudaMemcpyAsync(xn.data(), s->xnorm2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
         WUST_CUDA(cudaStreamSynchronize(st));
         check_tc_err(s);
-        double worst_err = 0, worst_res = 0;
+        double worst_err = 0, worst_res = 0, worst_rho = 0;
         for (int q = 0; q < S; ++q) {
             if (!(std::isfinite(rn[q]) && std::isfinite(dn[q]) && std::isfinite(xn[q])))
                 fail(WUST_ERR_NUMERICAL_FAILURE, "non-finite refinement residual");
             const double rho = rn_prev[q] > 0 ? std::sqrt(rn[q] / rn_prev[q]) : 0.0;
             const double rel_d = xn[q] > 0 ? std::sqrt(dn[q] / xn[q]) : 0.0;
             worst_err = std::fmax(worst_err, std::fmin(rho, 1.0) * rel_d);
+            worst_rho = std::fmax(worst_rho, rho);
             worst_res = std::fmax(worst_res, bn[q] > 0 ? std::sqrt(rn[q] / bn[q]) : std::sqrt(rn[q]));
         }
         s->last_refine_iters = k;
         s->last_residual = worst_res;
         s->last_error_est = worst_err;
         if (worst_err <= s->refine_tol) break;
+        if (worst_rho > kBf16Contraction) bf16_corr = false;
     }
     if (s->last_refine_iters == 1) refine_demote_launch(xa, out, s->plane() * S, st);   // out still holds x_0
 }
