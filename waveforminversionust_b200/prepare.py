@@ -184,3 +184,100 @@ def to_observations(obs: dict):
     from .objective import Observations
     return Observations(obs["x_m"], obs["y_m"], obs["tx_index"], obs["rx_index"], obs["frequencies_hz"], obs["Y"],
                         obs["mask"])
+
+
+def _axes_layout(a, axes: str):
+    """[tx, rx, frequency] from a declared axis order."""
+    if axes == "tx,rx,frequency":
+        return a
+    if axes == "frequency,tx,rx":
+        return np.moveaxis(a, 0, 2)
+    raise _invalid(f"Unsupported declared axes: {axes}")
+
+
+def wust_prepare_observations(inp: dict) -> dict:
+    """Canonical observations from a ``wust.frequency_input`` or a
+    ``wust.measurements`` artifact (wust_prepare_observations.m:1-109): the
+    geometry snapped to the grid (and, for canonical input, its sampling
+    indices checked against that), declared units and normalisation,
+    [tx, rx, frequency] layout, a 0/1 mask with masked values zeroed, the
+    Fourier sign brought to -1 (conjugation only for declared real
+    time-domain pressure) and ascending frequencies.  ``inp`` holds the
+    artifact's metadata, its arrays and the declared ``pressure_axes`` /
+    ``mask_axes`` of frequency input."""
+    schema = inp.get("schema")
+    if schema not in ("wust.frequency_input", "wust.measurements") or inp.get("schema_version") != 2:
+        raise WustError(1, "Expected a supported WUST v2 schema")
+    canonical = schema == "wust.measurements"
+    geo = wust_geometry(inp["grid"], inp["tx_xy_m"], inp["rx_xy_m"])
+    if canonical and not (np.array_equal(np.asarray(inp["tx_index"]).ravel().astype(np.int64), geo["tx_index"])
+                          and np.array_equal(np.asarray(inp["rx_index"]).ravel().astype(np.int64), geo["rx_index"])):
+        raise _invalid("Canonical sampling indices disagree with geometry")
+    f = np.asarray(inp["frequencies_hz"], np.float64).ravel()
+    if not (f.size and np.all(np.isfinite(f) & (f > 0)) and np.unique(f).size == f.size):
+        raise _invalid("Frequencies must be finite, positive and unique")
+    if inp.get("pressure_type") != "total_pressure":
+        raise _invalid("Ingestion requires total complex pressure, not scattered fields or ratios")
+    units, norm = inp.get("data_units"), inp.get("spectrum_normalization")
+    if units not in ("Pa*s", "instrument_units", "unknown") or norm not in ("dtft_dt", "discrete_sum", "unknown"):
+        raise _invalid("Explicit supported units and normalization required")
+    if units == "Pa*s" and norm != "dtft_dt":
+        raise _invalid("Pa*s requires the dt-weighted DTFT normalization")
+    nt, nr, nf = geo["tx_index"].size, geo["rx_index"].size, f.size
+    sign = inp.get("fourier_sign")
+    if canonical:
+        if not (np.isscalar(sign) and sign == -1 and np.all(np.diff(f) > 0)):
+            raise _invalid("Canonical observations require Fourier sign -1 and strictly increasing frequencies")
+        Y, mask = np.asarray(inp["Y"]), np.asarray(inp["mask"])
+        p_axes = m_axes = "tx,rx,frequency"
+    else:
+        p_axes, m_axes = inp["pressure_axes"], inp["mask_axes"]
+        Y = _axes_layout(np.asarray(inp["pressure"]), p_axes)
+        mask = np.asarray(inp["mask"])
+        if m_axes == "tx,rx":
+            if mask.shape != (nt, nr):
+                raise _invalid("Mask shape mismatch")
+            mask = np.repeat(mask[:, :, None], nf, axis=2)
+        else:
+            mask = _axes_layout(mask, m_axes)
+    if Y.ndim == 2:
+        Y = Y[:, :, None]
+    if mask.ndim == 2:
+        mask = mask[:, :, None]
+    if Y.dtype not in (np.complex64, np.complex128) or Y.shape != (nt, nr, nf):
+        raise _invalid("Pressure axes/shape mismatch")
+    if mask.shape != (nt, nr, nf) or not np.all((mask == 0) | (mask == 1)):
+        raise _invalid("Mask must contain only booleans/0/1")
+    mask = mask.astype(bool)
+    if not (mask.any() and np.all(np.isfinite(Y[mask]))):
+        raise _invalid("Empty observations or nonfinite pressure on a valid channel")
+    Y = Y.copy()
+    Y[~mask] = 0
+    order = np.arange(nf)
+    conversion = "none"
+    if not canonical:
+        if not (np.isscalar(sign) and sign in (-1, 1)):
+            raise _invalid("Declare Fourier sign -1 or +1; unknown conventions are rejected")
+        if sign == 1:
+            if inp.get("real_pressure") is not True:
+                raise _invalid("Conjugation requires declared real time-domain pressure")
+            Y = np.conj(Y)
+            conversion = "conjugate"
+        order = np.argsort(f, kind="stable")
+        Y, mask = Y[:, :, order], mask[:, :, order]
+    obs = dict(geo)
+    obs.update(schema="wust.measurements", schema_version=2, Y=Y, mask=mask, frequencies_hz=f[order], fourier_sign=-1,
+               shape_yx=(geo["y_m"].size, geo["x_m"].size), n_tx=nt, n_rx=nr,
+               valid_receiver_counts=mask.sum(axis=1),
+               frequency_data_norm=np.sum(np.abs(Y.astype(np.complex128)) ** 2, axis=(0, 1)),
+               grid=inp["grid"], data_units=units, spectrum_normalization=norm, pressure_type="total_pressure")
+    if canonical and "preparation" in inp:
+        obs["preparation"] = inp["preparation"]
+    else:
+        obs["preparation"] = dict(input_fourier_sign=sign, conversion=conversion, input_frequencies_hz=f,
+                                  canonical_to_input_permutation_1based=order + 1, input_pressure_axes=p_axes,
+                                  input_mask_axes=m_axes, phase_correction="none",
+                                  masked_values_policy="zero_after_preserving_mask",
+                                  input_precision="single" if Y.dtype == np.complex64 else "double",
+                                  measurement_provenance=inp.get("measurement_provenance", "unknown"))
+    return obs
