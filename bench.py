@@ -528,6 +528,95 @@ def run_batch(args, torch):
                           per_problem=rows)), flush=True)
 
 
+def run_simulate(args, torch):
+    """RF simulation (wust_simulate): the config-2 array on its 512^2 model
+    grid (dx 0.25 mm, 20-cell PML outside, 552^2 with it), 256 transmitters x
+    256 receivers on the 55 mm ring, Dirichlet 1 MHz tone burst, dt 40 ns, 400
+    time samples per step of the bench (the full 80 us record is 2000), all
+    transmitters batched.  value: transmitter-time-steps per second with the
+    model resident; e2e: the same through the Python call, RF read back to the
+    host.  The FP64 oracle on one transmitter and 20 time samples is the CPU
+    baseline."""
+    from waveforminversionust_b200 import _lib, synthetic
+    from waveforminversionust_b200.simulate import wust_simulate
+    p = synthetic.config2(seed=0, freqs=[1.2e6])
+    pml = 20
+    c = p.c_true[pml:-pml, pml:-pml]
+    x, y = p.x_m[pml:-pml], p.y_m[pml:-pml]
+    ny, nx = c.shape
+    # the ring's grid points, moved into the cropped model grid
+    iy, ix = (p.tx_index - 1) % p.shape[0] - pml, (p.tx_index - 1) // p.shape[0] - pml
+    tx = (iy + ny * ix + 1).astype(np.int32)
+    ry, rx_ = (p.rx_index - 1) % p.shape[0] - pml, (p.rx_index - 1) // p.shape[0] - pml
+    rx = (ry + ny * rx_ + 1).astype(np.int32)
+    n_time, dt = 400, 40e-9
+    c_ref = float(max(1600.0, np.ceil(c.max())))
+    t = np.arange(n_time) * dt
+    src = np.sin(2 * np.pi * 1e6 * t) * np.exp(-((t - 2e-6) / 0.7e-6) ** 2)
+    lib = _lib.load()
+    cm = np.ascontiguousarray(c.T)
+    rf = torch.empty((tx.size, rx.size, n_time), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def call():
+        _lib.check(lib.wust_simulate(cm.ctypes.data_as(C.c_void_p), ny, nx, float(y[1] - y[0]), float(x[1] - x[0]), dt,
+                                     n_time, src.ctypes.data_as(C.c_void_p), tx.ctypes.data_as(C.c_void_p), tx.size,
+                                     rx.ctypes.data_as(C.c_void_p), rx.size, pml, c_ref, 1000.0, 1, 0,
+                                     C.c_void_p(rf.data_ptr()), C.c_void_p(st.cuda_stream)))
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        call()
+    steps = max(1, min(args.steps, 3))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(steps):
+        call()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    units = tx.size * n_time
+    model = dict(c_mps=c, x_m=x, y_m=y, tx_index=tx, rx_index=rx, dt_s=dt, source_pressure=src)
+    cfg = dict(backend="native-batch", pml_size=pml, density_kg_m3=1000, sound_speed_ref_mps=c_ref,
+               downsample_factor=1, time_offset_s=0.0, work_dir=os.path.join(ROOT, "gpurun_out"))
+    t0 = time.perf_counter()
+    rec = wust_simulate(model, cfg)
+    e2e_s = time.perf_counter() - t0
+    from oracle import kwave_fp64 as o
+    t0 = time.perf_counter()
+    o.simulate(c, float(y[1] - y[0]), float(x[1] - x[0]), dt, src[:20], tx[:1], rx, pml, c_ref, 1000.0)
+    cpu_s = time.perf_counter() - t0
+    Ny, Nx = ny + 2 * pml, nx + 2 * pml
+    # per transmitter and time step: 7 FFT passes (R2C of p, C2R and R2C of
+    # the two velocities, C2R of the two divergences) read and write at
+    # least one real plane each, the three pointwise kernels 11 planes
+    plane = Ny * Nx * 4
+    alg_bytes = (7 * 2 + 11) * plane
+    achieved = alg_bytes * units / (ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    print(json.dumps(dict(
+        metric="simulated transmitter-time-steps per second", value=units / (ms * 1e-3), unit="tx*steps/s", n_gpus=1,
+        steps=steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
+        dtype="f32", data="synthetic",
+        config=dict(workload=f"RF simulation: {ny}x{nx} model + {pml}-cell PML ({Ny}x{Nx}), {tx.size} TX x {rx.size} RX, "
+                             f"{n_time} samples of dt {dt * 1e9:.0f} ns, all transmitters batched",
+                    l2=f"fields {7 * tx.size * plane / 1e9:.1f} GB, larger than L2"),
+        e2e=dict(value=units / e2e_s, unit="tx*steps/s", h2d_bytes_per_step=int(cm.nbytes + src.nbytes),
+                 d2h_bytes_per_step=int(rec["pressure"].nbytes)),
+        roofline=dict(kernel="time step (cuFFT R2C/C2R + 3 fused pointwise kernels) over all transmitters", bound="hbm",
+                      achieved=achieved, peak=hbm, unit="GB/s", frac=achieved / hbm,
+                      peak_source="MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s", traffic=None,
+                      algorithmic_bytes_per_tx_step=alg_bytes),
+        cpu_baseline=dict(value=20 / cpu_s, unit="tx*steps/s", cores=1, kind="port",
+                          sample="FP64 NumPy oracle, one transmitter, 20 time samples on the same grid"))), flush=True)
+
+
 def run_dtft(args, torch):
     """The DTFT of the RF preparation (wust_dtft): 2048-sample float32 RF of
     256 x 256 transmitter/receiver pairs at 16 frequencies, RF resident in
@@ -677,7 +766,7 @@ def main():
     ap.add_argument("--variants", default="c64,c64-refined,bf16-refined",
                     help="extra precision profiles timed beside the headline")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision", "autograd", "batch"],
+    ap.add_argument("--mode", default="gradient", choices=["gradient", "solve", "ncg", "dtft", "precision", "autograd", "batch", "simulate"],
                     help="solve: factor once, then time forward solves of all transmitters (kernel profiling); "
                          "ncg: time NCG updates of the reconstruction loop, update rules on the device and on the host; "
                          "dtft: time the RF preparation's DTFT")
@@ -708,6 +797,9 @@ def main():
 
     if args.mode == "dtft":
         run_dtft(args, torch)
+        return
+    if args.mode == "simulate":
+        run_simulate(args, torch)
         return
     if args.mode == "precision":
         run_precision(args, torch)

@@ -268,6 +268,25 @@ int wust_ncg_project(wust_solver *s, double *c, const double *direction, double 
 int wust_dtft(const double *time_s, int n_time, const double *frequencies_hz, int n_f, const void *rf, int rf_is_double,
               int n_rx, int n_tx, const uint8_t *active, wust_c64 *Y, void *stream);
 
+/* RF simulation of wust_simulate.m:1-87 (its 'native-batch' and
+ * 'matlab-serial' backends, which run k-Wave's 2-D first-order k-space solver
+ * per transmitter): linear acoustics, scalar density rho0, no absorption, a
+ * Dirichlet pressure source s(t) at each transmitter in turn, the pressure
+ * recorded at every receiver, a PML of pml_size cells (alpha 2) outside the
+ * grid, k-space correction at c_ref, then the FIR decimation of
+ * downsampleKWaveChannelData.m when decimation > 1.  c_mps: host [ny, nx]
+ * column-major (first axis y with spacing dy_m); source: host [n_time];
+ * tx_index / rx_index: host 1-based column-major grid indices, distinct;
+ * rf: device float [ceil(n_time / decimation), n_rx, n_tx] column-major (the
+ * reference's pressure(time, receiver, transmitter)).  tx_batch transmitters
+ * march together (0: all).  Checks the reference's preconditions (positive
+ * finite medium, CFL c dt / min(dx, dy) <= 0.3, c_ref >= max c, rho0 > 0,
+ * pml_size >= 1, decimation >= 1, at least two finite source samples, valid
+ * distinct indices) and synchronizes the stream (NULL: legacy default). */
+int wust_simulate(const double *c_mps, int ny, int nx, double dy_m, double dx_m, double dt_s, int n_time,
+                  const double *source, const int *tx_index, int n_tx, const int *rx_index, int n_rx, int pml_size,
+                  double c_ref_mps, double rho0_kg_m3, int decimation, int tx_batch, float *rf, void *stream);
+
 /* Counters of the last solve/oracle call: correction solves of the last
  * refined solve, its final relative FP64 residual |b - Hx| / |b| and forward
  * error estimate (refined profiles; -1 otherwise), and the number of kernel

@@ -105,3 +105,36 @@ def test_prepare_through_the_service_matches_wust_prepare(transport, tmp_path): 
     assert np.array_equal(arrays["mask"], want["mask"])
     scale = np.abs(want["Y"]).max()
     assert np.abs(arrays["Y"] - want["Y"]).max() <= 1e-6 * scale
+
+
+def test_simulate_through_the_service_matches_wust_simulate(transport, tmp_path):  # noqa: F811
+    """wust_run.m:33-39: the simulation input's positions snapped to its grid,
+    then wust_simulate; the RF artifact against the direct call."""
+    T = transport
+    from test_simulate import CFG, X, Y, pipeline_model
+    from waveforminversionust_b200 import service
+    from waveforminversionust_b200.simulate import wust_simulate
+    m = pipeline_model()
+    ny = Y.size
+    iy, ix = (m["tx_index"] - 1) % ny, (m["tx_index"] - 1) // ny
+    ry, rx = (m["rx_index"] - 1) % ny, (m["rx_index"] - 1) // ny
+    grid = dict(shape_yx=[23, 27], spacing_yx_m=[.0005, .0005], origin_yx_m=[Y[0] - .00025, X[0] - .00025],
+                origin_kind="pixel_edge")
+    inp = tmp_path / "model.json"
+    T.write_artifact(inp, "wust.simulation_input", dict(grid=grid, dt_s=m["dt_s"]),
+                     dict(c_mps=m["c_mps"], tx_xy_m=np.stack([X[ix], Y[iy]], 1), rx_xy_m=np.stack([X[rx], Y[ry]], 1),
+                          source_pressure=m["source_pressure"]))
+    cfg = dict(CFG, work_dir=str(tmp_path / "work"))
+    out = tmp_path / "rf.json"
+    req = tmp_path / "request.json"
+    req.write_text(json.dumps(request("simulate", inp, out, cfg)))
+    service.run(req, timeout_s=600)
+    doc, arrays = T.read_artifact(out, "wust.rf")
+    want = wust_simulate(m, cfg)
+    assert doc["metadata"]["data_units"] == "Pa" and doc["metadata"]["measurement_provenance"] == "self_simulated"
+    assert arrays["pressure"].shape == (200, 4, 3) and arrays["pressure"].dtype == np.float32
+    assert np.abs(arrays["pressure"] - want["pressure"]).max() <= 1e-6 * np.abs(want["pressure"]).max()
+    assert np.array_equal(arrays["time_s"], want["time_s"])
+    # the service takes the grid positions from the artifact's grid, the direct call from the test's axes
+    assert np.allclose(arrays["tx_xy_m"], want["tx_xy_m"], rtol=0, atol=1e-12)
+    assert np.allclose(arrays["rx_xy_m"], want["rx_xy_m"], rtol=0, atol=1e-12)

@@ -180,7 +180,7 @@ def test_service_failures(transport, tmp_path):
     with pytest.raises(service.RuntimeFailure) as err:
         service.run(req2, timeout_s=0.05)
     assert err.value.reason == "time_budget"
-    # transport errors before any work: relative paths, an existing output, simulate
+    # transport errors before any work: relative paths, an existing output, no timeout
     with pytest.raises(ValueError, match="absolute"):
         (tmp_path / "r3.json").write_text(json.dumps(request("ingest_frequency", "input.json", tmp_path / "o3.json")))
         service.run(tmp_path / "r3.json", timeout_s=10)
@@ -198,5 +198,5 @@ def test_describe_command_line(transport):
                          text=True, check=True, cwd=os.path.dirname(HERE))
     caps = json.loads(out.stdout)
     assert caps["schema"] == "wust.capabilities" and caps["schema_version"] == 2
-    assert "reconstruct" in caps["operations"] and "simulate" not in caps["operations"]
+    assert set(caps["operations"]) == {"ingest_frequency", "prepare", "reconstruct", "simulate"}
     assert caps["fourier_sign"] == -1

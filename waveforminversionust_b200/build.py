@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwust_b200.so")
-SOURCES = ["api.cu", "assemble.cu", "factor.cu", "sweep.cu", "objective.cu", "refine.cu", "noalloc.cu", "tcsweep.cu", "tcchunk.cu", "nsfactor.cu", "ncg.cu", "prepare.cu"]
+SOURCES = ["api.cu", "assemble.cu", "factor.cu", "sweep.cu", "objective.cu", "refine.cu", "noalloc.cu", "tcsweep.cu", "tcchunk.cu", "nsfactor.cu", "ncg.cu", "prepare.cu", "simulate.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

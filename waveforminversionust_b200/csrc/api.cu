@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include <cufft.h>
@@ -407,7 +408,14 @@ static void check_tc_err(wust_solver *s) {
 // rho_k = |r_k| / |r_{k-1}| is the contraction of one step, so
 // |e_k| / |x_k| ~ rho_k |d_k| / |x_k|.  Refinement stops when that estimate is
 // below refine_tol for every source (the residual alone is already small for
-// the unrefined c64 solution while its error is not).
+// the unrefined c64 solution while its error is not).  In the bf16-refined
+// profile the estimate is taken with a margin of 1.5: residual and error
+// contract at different rates there, and on the textured 552^2 medium the
+// true error of an adjoint solve was 1.17 times the estimate.  With a TF32
+// first sweep (tf32-refined) the estimate has stayed above the measured error
+// at 552^2 (errors of 1.5-2.8e-6 where refinement stopped below 1e-5), and a
+// margin there adds a correction sweep on the homogeneous medium (measured:
+// 100 ms per gradient instead of 85).
 static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, float2 *out) {
     cudaStream_t st = s->st;
     run_sweep(s, src, S, adjoint, out, s->bf16_all);
@@ -467,7 +475,8 @@ static void solve_into(wust_solver *s, const SrcView &src, int S, bool adjoint, 
         s->last_refine_iters = k;
         s->last_residual = worst_res;
         s->last_error_est = worst_err;
-        if (worst_err <= s->refine_tol) break;
+        const double margin = s->bf16_all ? 1.5 : 1.0;
+        if (margin * worst_err <= s->refine_tol) break;
         if (worst_rho > kBf16Contraction) bf16_corr = false;
     }
     if (s->last_refine_iters == 1) refine_demote_launch(xa, out, s->plane() * S, st);   // out still holds x_0
@@ -1139,6 +1148,42 @@ int wust_dtft(const double *time_s, int n_time, const double *frequencies_hz, in
         WUST_CUDA(cudaFreeAsync(bad, st));
         WUST_CUDA(cudaStreamSynchronize(st));
         if (h_bad) fail(WUST_ERR_INVALID_INPUT, "Nonfinite RF on an active channel");
+    });
+}
+
+int wust_simulate(const double *c_mps, int ny, int nx, double dy_m, double dx_m, double dt_s, int n_time,
+                  const double *source, const int *tx_index, int n_tx, const int *rx_index, int n_rx, int pml_size,
+                  double c_ref_mps, double rho0_kg_m3, int decimation, int tx_batch, float *rf, void *stream) {
+    return guarded([&] {
+        if (!c_mps || !source || !tx_index || !rx_index || !rf) fail(WUST_ERR_INVALID_INPUT, "simulate arguments missing");
+        if (ny < 1 || nx < 1 || n_tx < 1 || n_rx < 1) fail(WUST_ERR_INVALID_INPUT, "Invalid medium");
+        // wust_simulate.m:17-37
+        double cmax = 0.0;
+        for (size_t i = 0; i < (size_t)ny * nx; ++i) {
+            if (!(std::isfinite(c_mps[i]) && c_mps[i] > 0)) fail(WUST_ERR_INVALID_INPUT, "Invalid medium");
+            cmax = std::max(cmax, c_mps[i]);
+        }
+        if (!(dx_m > 0 && dy_m > 0 && std::isfinite(dx_m) && std::isfinite(dy_m)))
+            fail(WUST_ERR_INVALID_INPUT, "Uniform grid required");
+        if (!(dt_s > 0 && cmax * dt_s / std::min(dx_m, dy_m) <= 0.3)) fail(WUST_ERR_INVALID_INPUT, "CFL exceeds tested 0.3");
+        if (!(rho0_kg_m3 > 0 && std::isfinite(rho0_kg_m3) && c_ref_mps >= cmax && std::isfinite(c_ref_mps)))
+            fail(WUST_ERR_INVALID_INPUT, "Invalid density or reference speed");
+        if (decimation < 1) fail(WUST_ERR_INVALID_INPUT, "Invalid decimation factor");
+        if (pml_size < 1) fail(WUST_ERR_INVALID_INPUT, "Positive integer outside PML required");
+        if (n_time < 2) fail(WUST_ERR_INVALID_INPUT, "Finite source waveform required");
+        for (int t = 0; t < n_time; ++t)
+            if (!std::isfinite(source[t])) fail(WUST_ERR_INVALID_INPUT, "Finite source waveform required");
+        for (const int *ids : {tx_index, rx_index}) {
+            const int n = ids == tx_index ? n_tx : n_rx;
+            std::vector<int> v(ids, ids + n);
+            std::sort(v.begin(), v.end());
+            for (int i = 0; i < n; ++i)
+                if (v[i] < 1 || (long long)v[i] > (long long)nx * ny || (i > 0 && v[i] == v[i - 1]))
+                    fail(WUST_ERR_INVALID_INPUT, "Invalid/duplicate array indices");
+        }
+        SimulateArgs a{c_mps, ny, nx, dy_m, dx_m, dt_s, n_time, source, tx_index, n_tx, rx_index, n_rx, pml_size,
+                       c_ref_mps, rho0_kg_m3, decimation, tx_batch};
+        simulate_rf(a, rf, static_cast<cudaStream_t>(stream));
     });
 }
 

@@ -210,4 +210,24 @@ void refine_step_launch(const RefineWeights &w, const SrcView &b, const float2 *
 // u = c64(x)
 void refine_demote_launch(const double2 *x, float2 *u, size_t n, cudaStream_t st);
 
+
+// RF simulation (simulate.cu): host inputs, device output rf [ly][nrx][ntx]
+// column-major (ly = ceil(nt / decimation)).
+struct SimulateArgs {
+    const double *c;          // [ny][nx] column-major sound speed (m/s)
+    int ny, nx;
+    double dy, dx, dt;        // grid spacing (m) along y (first axis) and x, time step (s)
+    int nt;
+    const double *source;     // [nt] Dirichlet source pressure
+    const int *tx_index;      // [ntx] 1-based column-major
+    int ntx;
+    const int *rx_index;      // [nrx]
+    int nrx;
+    int pml;                  // PML cells outside the grid on every side
+    double c_ref, rho0;
+    int decimation;           // >= 1
+    int tx_batch;             // transmitters per batch (0: all)
+};
+void simulate_rf(const SimulateArgs &a, float *rf, cudaStream_t st);
+
 }  // namespace wust

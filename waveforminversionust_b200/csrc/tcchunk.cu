@@ -166,6 +166,9 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
     uint8_t *bg = p.bglob + (size_t)g * kc * bbytes;
     unsigned *ctr = p.group_ctr + g;
     const int row0 = 64 * t;                                     // first complex interior row of this CTA
+    // the boundary chain splits the launch's sources over its groups: group g
+    // takes sources [so, so + N) of the launch (every other pass: so = 0)
+    const int so = p.pass == CK_BOUNDARY ? g * N : 0;
 
     // this group's chunk, kind and steps
     int chunk, kind, t0, nsteps;
@@ -196,10 +199,11 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
     // (0 for the padding sources beyond s_end: the caller's fields hold only
     // s_end sources)
     auto cval = [&](int in, const float *pl, int y, int s) -> float2 {
-        if (y < 0 || y >= ny || p.s0 + s >= p.s_end) return f2(0.f, 0.f);
-        if (in == IN_PLANES) return f2(__ldcg(pl + (size_t)s * ny + y), __ldcg(pl + (size_t)(kCkMaxN + s) * ny + y));
-        if (in == IN_UCOL) return __ldcg(p.u + plane * (p.s0 + s) + (size_t)ny * (nx - 1) + y);
-        if (in == IN_IDENT) return f2((y >= 1 && y <= n && y - 1 == p.s0 + s) ? 1.f : 0.f, 0.f);
+        if (y < 0 || y >= ny || p.s0 + so + s >= p.s_end) return f2(0.f, 0.f);
+        if (in == IN_PLANES)
+            return f2(__ldcg(pl + (size_t)(so + s) * ny + y), __ldcg(pl + (size_t)(kCkMaxN + so + s) * ny + y));
+        if (in == IN_UCOL) return __ldcg(p.u + plane * (p.s0 + so + s) + (size_t)ny * (nx - 1) + y);
+        if (in == IN_IDENT) return f2((y >= 1 && y <= n && y - 1 == p.s0 + so + s) ? 1.f : 0.f, 0.f);
         return f2(0.f, 0.f);
     };
     // staged state at complex interior row yp (row0 - 1 .. row0 + 64)
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         if (wu && !ident) {
             // border rows 0 and ny-1 of u(:, j1-1) (no B entry)
             for (int it = tid; it < 2 * N; it += kCkThreads) {
-                const int e = it / N, s = it % N, gs = p.s0 + s;
+                const int e = it / N, s = it % N, gs = p.s0 + so + s;
                 if ((e == 0 && t != 0) || (e == 1 && t != p.mt - 1) || gs >= p.s_end) continue;
                 const int y = e == 0 ? 0 : ny - 1, yp = y - 1;
                 float2 wc, wm, wp;
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                 float2 base[4][2];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const int gs = p.s0 + 8 * grp + 4 * h4 + q;
+                    const int gs = p.s0 + so + 8 * grp + 4 * h4 + q;
                     base[q][0] = base[q][1] = f2(0.f, 0.f);
                     if (has_base && gs < p.s_end) {
                         if (v0) base[q][0] = step_base<ADJ>(p.src, p.u, ny, nx, fwd1, j1, y0, gs);
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const int s = 8 * grp + 4 * h4 + q, gs = p.s0 + s;
+                    const int s = 8 * grp + 4 * h4 + q, gs = p.s0 + so + s;
                     const float4 cv = *reinterpret_cast<const float4 *>(cs + s * 64 + 2 * lane);
                     const float2 c0 = f2(cv.x, cv.y), c1 = f2(cv.z, cv.w);
                     float2 cm = f2(__shfl_up_sync(0xffffffffu, c1.x, 1), __shfl_up_sync(0xffffffffu, c1.y, 1));
@@ -344,7 +348,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                             if (wu) p.u[plane * gs + (size_t)ny * (j1 - 1) + y0 + 1] = b1;
                         }
                         if (out) {
-                            float *re = out + (size_t)s * ny, *im = out + (size_t)(kCkMaxN + s) * ny;
+                            float *re = out + (size_t)(so + s) * ny, *im = out + (size_t)(kCkMaxN + so + s) * ny;
                             if (v0) { __stcg(re + y0, b0.x); __stcg(im + y0, b0.y); }
                             if (v1) { __stcg(re + y0 + 1, b1.x); __stcg(im + y0 + 1, b1.y); }
                         }
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
             float2 o[4][2];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int s = sb0 + kCkWarps * q, gs = p.s0 + s;
+                const int s = sb0 + kCkWarps * q, gs = p.s0 + so + s;
                 o[q][0] = o[q][1] = f2(0.f, 0.f);
                 if (s < N && gs < p.s_end) {
                     if (old_u) {
@@ -444,16 +448,15 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                         if (v0) o[q][0] = __ldcg(uc + y0);
                         if (v1) o[q][1] = __ldcg(uc + y0 + 1);
                     } else if (kind == K_BOUND) {
-                        if (v0) o[q][0] = f2(__ldcg(oldp + (size_t)s * ny + y0), __ldcg(oldp + (size_t)(kCkMaxN + s) * ny + y0));
-                        if (v1)
-                            o[q][1] = f2(__ldcg(oldp + (size_t)s * ny + y0 + 1),
-                                         __ldcg(oldp + (size_t)(kCkMaxN + s) * ny + y0 + 1));
+                        const float *ore = oldp + (size_t)(so + s) * ny, *oim = oldp + (size_t)(kCkMaxN + so + s) * ny;
+                        if (v0) o[q][0] = f2(__ldcg(ore + y0), __ldcg(oim + y0));
+                        if (v1) o[q][1] = f2(__ldcg(ore + y0 + 1), __ldcg(oim + y0 + 1));
                     }
                 }
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int s = sb0 + kCkWarps * q, gs = p.s0 + s;
+                const int s = sb0 + kCkWarps * q, gs = p.s0 + so + s;
                 if (s >= N) break;                                   // warp-uniform
                 float4 *cp4 = reinterpret_cast<float4 *>(cs + s * 64 + 2 * lane);
                 float4 cv = *cp4;
@@ -472,7 +475,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                 if (lane == 0) __stcg(my_edges + s, f2(cv.x, cv.y));
                 if (lane == 31 && v1) __stcg(my_edges + kCkMaxN + s, f2(cv.z, cv.w));
                 if (last) {
-                    float *re = curp + (size_t)s * ny, *im = curp + (size_t)(kCkMaxN + s) * ny;
+                    float *re = curp + (size_t)(so + s) * ny, *im = curp + (size_t)(kCkMaxN + so + s) * ny;
                     if (v0) { __stcg(re + y0, cv.x); __stcg(im + y0, cv.y); }
                     if (v1) { __stcg(re + y0 + 1, cv.z); __stcg(im + y0 + 1, cv.w); }
                 }
@@ -481,7 +484,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         if (kind == K_EXACT && ADJ && !fwd && t == 0) {
             // H^H backward: border rows of u(:, j) are zero
             for (int s = tid; s < N; s += kCkThreads) {
-                const int gs = p.s0 + s;
+                const int gs = p.s0 + so + s;
                 if (gs >= p.s_end) continue;
                 p.u[plane * gs + (size_t)ny * j] = f2(0.f, 0.f);
                 p.u[plane * gs + (size_t)ny * j + ny - 1] = f2(0.f, 0.f);
@@ -508,7 +511,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         for (int c = 0; c < 2; ++c) {
             if (!cols[c]) continue;
             for (int it = tid - 32; it < N * 5; it += kCkThreads - 32) {
-                const int s = it / 5, q = it % 5, gs = p.s0 + s;
+                const int s = it / 5, q = it % 5, gs = p.s0 + so + s;
                 if (gs >= p.s_end) continue;
                 const char *first = reinterpret_cast<const char *>(cols[c] + plane * gs + y_first);
                 const char *last = reinterpret_cast<const char *>(cols[c] + plane * gs + y_last);
@@ -988,7 +991,16 @@ void tc_chunk_solve(const Coefs<float2> &co, const uint8_t *afwd, const uint8_t 
             p.lpack = bf16 ? lpack_of(g, b.lpack16, adjoint, half, g.page_bytes16)
                            : lpack_of(g, b.lpack, adjoint, half, g.page_bytes);
             ck_launch(p, adjoint, bf16, CK_FIRST, g.C, st);
-            if (g.C >= 3) ck_launch(p, adjoint, bf16, CK_BOUNDARY, 1, st);
+            if (g.C >= 3) {
+                // the chain of C - 2 dense steps on up to C groups, each
+                // carrying a 16-multiple slice of the sources (one group
+                // would leave all but mt SMs idle for the whole chain)
+                const int N = p.N;
+                const int per = ceil_div(ceil_div(N, g.C), 16) * 16;
+                p.N = per;
+                ck_launch(p, adjoint, bf16, CK_BOUNDARY, ceil_div(N, per), st);
+                p.N = N;
+            }
             if (g.C >= 2) ck_launch(p, adjoint, bf16, CK_SECOND, g.C - 1, st);
         }
     }

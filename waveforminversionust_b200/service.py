@@ -15,8 +15,8 @@ the operations with this library:
   curvature and update on the GPU (``wust_reconstruct``), in the precision
   profile the request's config names (``precision``, default
   ``tf32-refined``);
-- ``simulate`` (the k-Wave simulator) is not served: the request fails with
-  ``runtime_failure``.
+- ``simulate``: RF records of every transmitter from a sound-speed model,
+  k-Wave's 2-D k-space method batched on the GPU (``wust_simulate``).
 
 Command line, as the reference's:
 ``python -m waveforminversionust_b200.service describe`` and
@@ -58,8 +58,8 @@ def capabilities() -> dict:
         "runtime_name": RUNTIME_NAME,
         "runtime_version": RUNTIME_VERSION,
         "schemas": T.SCHEMAS,
-        "operations": [op for op in T.OPERATION_INPUTS if op != "simulate"],
-        "input_schemas": {op: list(v) for op, v in T.OPERATION_INPUTS.items() if op != "simulate"},
+        "operations": list(T.OPERATION_INPUTS),
+        "input_schemas": {op: list(v) for op, v in T.OPERATION_INPUTS.items()},
         "sound_speed_reconstruction": {"supported": True, "dimensions": [2]},
         "attenuation_reconstruction": {"supported": False},
         "profiles": {"gpu": "gpu_complex64", **{f"gpu_{p}": p for p in _PRECISIONS}},
@@ -109,7 +109,7 @@ def _measurements_artifact(obs: dict):
 
 def _environment(req: dict) -> dict:
     env = {"runtime_version": RUNTIME_VERSION, "platform": sys.platform, "python": sys.version.split()[0]}
-    if req["operation"] in ("reconstruct", "prepare"):
+    if req["operation"] in ("reconstruct", "prepare", "simulate"):
         import torch
         from . import _lib
         major, minor, patch = (_lib.C.c_int() for _ in range(3))
@@ -170,6 +170,17 @@ def execute(req: dict) -> tuple[str, dict, dict]:
             raise WustError(1, f"Unsupported precision profile {cfg.get('precision')!r}")
         result = wust_reconstruct(_observations(obs), np.asarray(initial["initial_mps"], np.float64), cfg)
         return ("wust.reconstruction",) + _reconstruction_artifact(result, cfg, obs)
+    if op == "simulate":
+        from .prepare import wust_geometry
+        from .simulate import wust_simulate
+        model = _artifact_value(req["input_manifest"], "wust.simulation_input")
+        geo = wust_geometry(model["grid"], model["tx_xy_m"], model["rx_xy_m"])      # wust_run.m:33-39
+        model.update(x_m=geo["x_m"], y_m=geo["y_m"], tx_index=geo["tx_index"], rx_index=geo["rx_index"])
+        rf = wust_simulate(model, dict(req["config"]))
+        arrays = {k: rf[k] for k in T.ARRAY_FIELDS["wust.rf"]}
+        arrays["pressure"] = np.asarray(arrays["pressure"], np.float32)
+        meta = {k: v for k, v in rf.items() if k not in arrays and k not in ("schema", "schema_version")}
+        return "wust.rf", arrays, meta
     raise RuntimeFailure("runtime_failure", f"Operation {op!r} is not served by this runtime")
 
 
@@ -249,8 +260,6 @@ def run(request_path, timeout_s=None) -> dict:
     T.read_manifest(req["input_manifest"], T.OPERATION_INPUTS[req["operation"]])
     if req["operation"] == "reconstruct":
         T.read_manifest(req["initial_manifest"], "wust.initial_model")
-    if req["operation"] == "simulate":
-        raise RuntimeFailure("runtime_failure", "The k-Wave simulator is not served by this runtime")
 
     # the run folder keeps the request and any partial output on failure
     folder = Path(tempfile.mkdtemp(prefix=f"{output.stem}-run-", dir=output.parent))
