@@ -41,6 +41,7 @@ namespace wust {
 constexpr int kCkThreads = 512;
 constexpr int kCkWarps = kCkThreads / 32;
 constexpr int kCkStages = 4;
+constexpr int kCopyTid = 96;                                     // the ring's copy thread (warp 3, lane 0)
 constexpr int kCkMaxN = 256;                                     // sources per launch (MMA N)
 constexpr int kCkRowsPerChunk = 16;                              // complex rows per K chunk (TF32)
 constexpr int kCkRowsPerChunk16 = 32;                            // complex rows per K chunk (BF16)
@@ -156,6 +157,7 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
     uint64_t *done = empty + kCkStages;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     int *s_ok = reinterpret_cast<int *>(tmem_slot + 1);
+    uint32_t *s_ring = reinterpret_cast<uint32_t *>(s_ok + 1);   // [0] A, [1] B copies issued, [2] full waits done
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = blockIdx.x / p.mt, t = blockIdx.x % p.mt;
@@ -523,37 +525,54 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
         }
     };
 
-    // ---- bulk-copy ring (thread 0); chunk ci = k * kc + q of step k --------
-    uint32_t a_next = 0, b_next = 0, retired = 0, full_waited = 0;
+    // ---- bulk-copy ring; chunk ci = k * kc + q of step k --------------------
+    // Two threads drive it: the copy thread (kCopyTid) refills each stage as
+    // soon as the MMAs that read it have completed, and thread 0 issues each
+    // chunk's MMAs as soon as its copies have landed, so neither waits on
+    // the other's latency.  A chunk's stage is slot ci % kCkStages, used for
+    // the (ci / kCkStages)-th time.
+    uint32_t a_next = 0, b_next = 0, full_waited = 0;
     // the page stream passes through L2 once; the packed B is read by every
     // CTA of the group and should stay
     const uint64_t a_policy = tc::policy_evict_first();
     const uint64_t b_policy = tc::policy_evict_last();
-    auto pump = [&](int k, bool b_ready) {
-        const uint32_t a_end = (uint32_t)min(k + 2, nsteps) * (uint32_t)kc;
-        while (a_next < a_end && a_next < retired + kCkStages) {
-            const int ks = (int)(a_next / kc), q = (int)(a_next % kc), slot = (int)(a_next % kCkStages);
-            tc::mbar_expect_tx(&full[slot], tc::kAChunk);
-            tc::bulk_g2s_hint(sA + (size_t)slot * tc::kAChunk, apage(ks) + ((size_t)t * kc + q) * tc::kAChunk,
-                              tc::kAChunk, &full[slot], a_policy);
-            ++a_next;
+    // copy thread: the A chunk a_next into its stage, once the MMAs of the
+    // chunk that used the stage before have completed
+    auto issue_a = [&]() -> bool {
+        const uint32_t c = a_next;
+        const int ks = (int)(c / kc), q = (int)(c % kc), slot = (int)(c % kCkStages);
+        if (c >= (uint32_t)kCkStages && !tc::mbar_wait(&empty[slot], ((c / kCkStages) - 1) & 1u, p.timeout_ns))
+            return false;
+        tc::mbar_expect_tx(&full[slot], tc::kAChunk);
+        tc::bulk_g2s_hint(sA + (size_t)slot * tc::kAChunk, apage(ks) + ((size_t)t * kc + q) * tc::kAChunk, tc::kAChunk,
+                          &full[slot], a_policy);
+        ++a_next;
+        return true;
+    };
+    // copy thread, step k: every B chunk of the step (each after its A
+    // chunk), then the next step's first A chunks as the stages free up
+    auto copies = [&](int k) {
+        bool good = true;
+        const uint32_t end = (uint32_t)(k + 1) * (uint32_t)kc;
+        while (good && b_next < end) {
+            if (a_next <= b_next && !(good = issue_a())) break;
+            const int q = (int)(b_next % kc), slot = (int)(b_next % kCkStages);
+            tc::mbar_expect_tx(&full[slot], (uint32_t)bbytes);
+            tc::bulk_g2s_hint(sB + (size_t)slot * kCkBSlot, bg + (size_t)q * bbytes, (uint32_t)bbytes, &full[slot],
+                              b_policy);
+            ++b_next;
         }
-        if (b_ready) {
-            const uint32_t b_end = (uint32_t)(k + 1) * (uint32_t)kc;
-            while (b_next < b_end && b_next < a_next) {
-                const int q = (int)(b_next % kc), slot = (int)(b_next % kCkStages);
-                tc::mbar_expect_tx(&full[slot], (uint32_t)bbytes);
-                tc::bulk_g2s_hint(sB + (size_t)slot * kCkBSlot, bg + (size_t)q * bbytes, (uint32_t)bbytes, &full[slot],
-                                  b_policy);
-                ++b_next;
-            }
-        }
+        const uint32_t a_end = min((uint32_t)min(k + 2, nsteps) * (uint32_t)kc, end + (uint32_t)kCkStages);
+        while (good && a_next < a_end) good = issue_a();
+        if (!good) atomicCAS(p.err, 0, SITE_COPY);
     };
 
     unsigned epoch = 0;
     bool ok = nsteps > 0;
     if (ok) {
-        if (tid == 0) pump(0, false);
+        if (tid == kCopyTid)                                // the first A chunks of step 0
+            while (a_next < (uint32_t)min(kCkStages, kc) && issue_a()) {
+            }
         int in0 = IN_ZERO, mode0 = P_STENCIL;
         const float *pl0 = nullptr;
         if (kind == K_EXACT && chunk > 0) {
@@ -586,8 +605,8 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
 #endif
     for (int k = 0; k < nsteps && ok; ++k) {
         CPROF(6);
+        if (tid == kCopyTid) copies(k);
         if (tid == 0) {
-            pump(k, true);
             bool good = true;
             for (int q = 0; q < kc; ++q) {
                 const uint32_t ci = (uint32_t)k * kc + q;
@@ -601,29 +620,11 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                                   tc::smem_desc(sB + (size_t)slot * kCkBSlot + kk * 256), idesc,
                                   (q > 0 || kk > 0) ? 1u : 0u);
                 tc::commit(&empty[slot]);
-                if (q >= 1) {
-                    const uint32_t pc = ci - 1;
-                    if (!tc::mbar_wait(&empty[pc % kCkStages], (pc / kCkStages) & 1u, p.timeout_ns)) {
-                        good = false;
-                        break;
-                    }
-                    retired = ci;
-                    pump(k, true);
-                }
             }
             tc::commit(done);
-            if (good) {
-                const uint32_t pc = (uint32_t)(k + 1) * kc - 1;
-                if (tc::mbar_wait(&empty[pc % kCkStages], (pc / kCkStages) & 1u, p.timeout_ns)) {
-                    retired = pc + 1;
-                    pump(k, true);          // A chunks of the next step
-                } else {
-                    good = false;
-                }
-            }
             if (!good) atomicCAS(p.err, 0, SITE_COPY);
         }
-        if (warp >= 1) prefetch_cols(k);
+        if (warp >= 1 && tid != kCopyTid) prefetch_cols(k);
         if (warp == 1 || warp == 2) {
             const bool next_b = k + 1 < nsteps || (ADJ && p.pass == CK_FIRST && chunk + 1 < p.C);
             if (next_b) {
@@ -676,10 +677,16 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
 
     // copies issued but never waited for (a failure): stand in for the B
     // copies that will not come, then let them land (bounded)
+    if (tid == kCopyTid) {
+        s_ring[0] = a_next;
+        s_ring[1] = b_next;
+    }
+    if (tid == 0) s_ring[2] = full_waited;
+    __syncthreads();
     if (tid == 0) {
-        for (uint32_t ci = full_waited; ci < a_next; ++ci) {
+        for (uint32_t ci = s_ring[2]; ci < s_ring[0]; ++ci) {
             const int slot = (int)(ci % kCkStages);
-            if (ci >= b_next) tc::mbar_arrive(&full[slot]);
+            if (ci >= s_ring[1]) tc::mbar_arrive(&full[slot]);
             tc::mbar_wait(&full[slot], (ci / kCkStages) & 1u, p.timeout_ns);
         }
     }
