@@ -63,6 +63,7 @@ constexpr int kStageBytes = tc::kAChunk + kBChunkNs;
 constexpr size_t kNsSmem = (size_t)kStages * kStageBytes + 512;
 static_assert(kNsSmem <= 232448, "shared memory of one CTA");
 constexpr int kTmemCols = 128;
+constexpr int kNsCopyTid = 96;                     // the ring's copy thread (warp 3, lane 0)
 
 constexpr float kAccept = 2e-4f;        // residual small enough: keep X_k
 // One more update, then accept: from the page's first residual (the
@@ -203,31 +204,38 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     tc::fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    uint32_t u_issue = 0, u_cons = 0;    // ring counters (thread 0)
+    uint32_t u_issue = 0, u_cons = 0;    // ring counters (copy thread, thread 0)
     uint32_t n_gemm = 0;                 // GEMMs run (done-barrier phase)
     bool ok = true;
 
     // One GEMM C = Apack * Bpack^T over this CTA's K slice into TMEM, then
-    // the partial tile into L2.  Returns false on an expired wait.
+    // the partial tile into L2.  Returns false on an expired wait.  The copy
+    // thread (kNsCopyTid) refills each stage as soon as the MMAs that read it
+    // have completed; thread 0 issues each chunk's MMAs as soon as its copies
+    // have landed.  Both count the chunks of every GEMM (u_issue, u_cons), so
+    // a stage's parity carries over from one GEMM to the next.
     auto gemm = [&](const uint8_t *Apack, const uint8_t *Bpack) -> bool {
         NSPROF(14);
-        if (tid == 0) {
+        if (tid == kNsCopyTid) {
             const uint8_t *ab = Apack + ((size_t)mt * p.kc + c0) * tc::kAChunk;
             const uint8_t *bb = Bpack + ((size_t)nb * p.kc + c0) * kBChunkNs;
             bool good = true;
-            auto issue = [&](int c) {
+            for (int c = 0; c < nch && good; ++c) {
                 const uint32_t s = u_issue % kStages, f = u_issue / kStages;
-                if (f >= 1 && !tc::mbar_wait(&empty[s], (f - 1) & 1u, p.timeout_ns)) good = false;
+                if (f >= 1 && !tc::mbar_wait(&empty[s], (f - 1) & 1u, p.timeout_ns)) {
+                    good = false;
+                    break;
+                }
                 uint8_t *st = smem + (size_t)s * kStageBytes;
                 tc::mbar_expect_tx(&full[s], kStageBytes);
                 tc::bulk_g2s(st, ab + (size_t)c * tc::kAChunk, tc::kAChunk, &full[s]);
                 tc::bulk_g2s(st + tc::kAChunk, bb + (size_t)c * kBChunkNs, kBChunkNs, &full[s]);
                 ++u_issue;
-            };
-            // kStages - 1 chunks ahead; chunk c + kStages - 1 refills the stage
-            // of chunk c - 1, whose MMAs were issued one chunk earlier
-            for (int c = 0; c < nch && c < kStages - 1; ++c) issue(c);
-            NSPROF(12);
+            }
+            if (!good) atomicCAS(p.err, 0, NS_SITE_COPY);
+        }
+        if (tid == 0) {
+            bool good = true;
             constexpr uint32_t kIdesc = tc::instr_desc<true>(tc::kTileRows, NTN);
             for (int c = 0; c < nch; ++c) {
                 const uint32_t s = u_cons % kStages, f = u_cons / kStages;
@@ -241,7 +249,6 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                     tc::mma<true>(tmem, tc::smem_desc(st + k * 256), tc::smem_desc(st + tc::kAChunk + k * 256), kIdesc,
                                   (c > 0 || k > 0) ? 1u : 0u);
                 tc::commit(&empty[s]);
-                if (c + kStages - 1 < nch) issue(c + kStages - 1);
             }
             tc::commit(done);
             if (!good) atomicCAS(p.err, 0, NS_SITE_COPY);
