@@ -530,7 +530,7 @@ def run_batch(args, torch):
 
 def run_simulate(args, torch):
     """RF simulation (wust_simulate): the config-2 array on its 512^2 model
-    grid (dx 0.25 mm, 20-cell PML outside, 552^2 with it), 256 transmitters x
+    grid (dx 0.25 mm, 32-cell PML outside, 576^2 with it), 256 transmitters x
     256 receivers on the 55 mm ring, Dirichlet 1 MHz tone burst, dt 40 ns, 400
     time samples per step of the bench (the full 80 us record is 2000), all
     transmitters batched.  value: transmitter-time-steps per second with the
@@ -540,14 +540,17 @@ def run_simulate(args, torch):
     from waveforminversionust_b200 import _lib, synthetic
     from waveforminversionust_b200.simulate import wust_simulate
     p = synthetic.config2(seed=0, freqs=[1.2e6])
-    pml = 20
-    c = p.c_true[pml:-pml, pml:-pml]
-    x, y = p.x_m[pml:-pml], p.y_m[pml:-pml]
+    hpml = 20                                  # the Helmholtz grid's PML, cropped off
+    c = p.c_true[hpml:-hpml, hpml:-hpml]
+    x, y = p.x_m[hpml:-hpml], p.y_m[hpml:-hpml]
+    # the k-space PML outside the 512^2 model: 32 cells make the FFT grid
+    # 576^2 = 2^6 3^2 (k-Wave's advice: FFT sizes of small primes)
+    pml = 32
     ny, nx = c.shape
     # the ring's grid points, moved into the cropped model grid
-    iy, ix = (p.tx_index - 1) % p.shape[0] - pml, (p.tx_index - 1) // p.shape[0] - pml
+    iy, ix = (p.tx_index - 1) % p.shape[0] - hpml, (p.tx_index - 1) // p.shape[0] - hpml
     tx = (iy + ny * ix + 1).astype(np.int32)
-    ry, rx_ = (p.rx_index - 1) % p.shape[0] - pml, (p.rx_index - 1) // p.shape[0] - pml
+    ry, rx_ = (p.rx_index - 1) % p.shape[0] - hpml, (p.rx_index - 1) // p.shape[0] - hpml
     rx = (ry + ny * rx_ + 1).astype(np.int32)
     n_time, dt = 400, 40e-9
     c_ref = float(max(1600.0, np.ceil(c.max())))
