@@ -26,6 +26,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -581,7 +582,7 @@ def run_simulate(args, torch):
     units = tx.size * n_time
     model = dict(c_mps=c, x_m=x, y_m=y, tx_index=tx, rx_index=rx, dt_s=dt, source_pressure=src)
     cfg = dict(backend="native-batch", pml_size=pml, density_kg_m3=1000, sound_speed_ref_mps=c_ref,
-               downsample_factor=1, time_offset_s=0.0, work_dir=os.path.join(ROOT, "gpurun_out"))
+               downsample_factor=1, time_offset_s=0.0, work_dir=tempfile.mkdtemp(prefix="wust-sim-"))
     t0 = time.perf_counter()
     rec = wust_simulate(model, cfg)
     e2e_s = time.perf_counter() - t0
