@@ -311,6 +311,14 @@ int wust_solver_sweep_times(const wust_solver *s, double *total_ms, long long *c
  * WUST_PRECISION_TF32_REFINED report {0, 0, 0, Nx}. */
 int wust_solver_factor_stats(const wust_solver *s, long long out[4]);
 
+/* How the last factorization ran its Newton-Schulz pages (no counterpart in
+ * the reference): *k_slices the K split of each GEMM tile (0: no Newton-Schulz
+ * pages for this profile or grid), *cluster 1 if the K slices of a tile ran as
+ * one thread-block cluster (split-K partials summed through distributed
+ * shared memory), 0 if as separate CTAs (partials through L2), -1 if no
+ * Newton-Schulz launch ran.  Either pointer may be NULL. */
+int wust_solver_factor_info(const wust_solver *s, int *k_slices, int *cluster);
+
 /* Self-test of the bounded device-side wait used by the persistent kernels
  * (no counterpart in the reference, whose MEX calls are synchronous library
  * calls): one CTA waits at a grid barrier that can never fill; the wait must

@@ -290,6 +290,41 @@ def test_newton_schulz_factor_agrees_with_gauss_jordan():
     tc.close()
 
 
+def test_newton_schulz_cluster_kernel_matches_classic_kernel(monkeypatch):
+    """The Newton-Schulz kernel launched as clusters (the K slices of a tile
+    sum their split-K partials through distributed shared memory) gives the
+    same Schur inverses, bit for bit, as the kernel whose partials go through
+    L2 (same K split, same summation order), with the same page decisions,
+    on a textured grid where pages take the cubic, quadratic and Gauss-Jordan
+    routes."""
+    from waveforminversionust_b200.solver import HelmholtzSolver
+    ny = nx = 482                     # 480 interior rows: 8 x 5 tiles, K split 3 either way
+    dx = 0.3e-3
+    x = (np.arange(nx) - (nx - 1) / 2) * dx
+    y = (np.arange(ny) - (ny - 1) / 2) * dx
+    X, Y = np.meshgrid(x, y)
+    rng = np.random.default_rng(11)
+    c = 1500 + 60 * np.exp(-((X - 4e-3) ** 2 + Y ** 2) / (2 * (20e-3) ** 2)) + 5 * rng.standard_normal(X.shape)
+    opts = dict(backend="gpu", stencil_bounds=(1400, 1700))
+    monkeypatch.setenv("WUST_NS_CLUSTER", "0")
+    classic = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, 16 * dx, opts, precision="tf32-refined",
+                              max_sources=4)
+    monkeypatch.delenv("WUST_NS_CLUSTER")
+    clustered = HelmholtzSolver(x, y, c, None, 0.8e6, -1, 10.0, 16 * dx, opts, precision="tf32-refined",
+                                max_sources=4)
+    ia, ib = classic.factor_info(), clustered.factor_info()
+    assert ia == {"k_slices": 3, "cluster": 0}, ia
+    assert ib == {"k_slices": 3, "cluster": 1}, ib
+    sa, sb = classic.factor_stats(), clustered.factor_stats()
+    assert sa == sb, (sa, sb)
+    assert sa["gemms"] > 2 * sa["newton_schulz_pages"], sa      # cubic / repeated updates were taken
+    a = to_np(classic.block("invT"))
+    b = to_np(clustered.block("invT"))
+    assert np.array_equal(np.ascontiguousarray(a).view(np.uint32), np.ascontiguousarray(b).view(np.uint32))
+    classic.close()
+    clustered.close()
+
+
 def test_mass_apply_matches_oracle(small):
     p, ref = small
     s = make_gpu_solver(p, p.c_true, p.frequencies_hz[0])

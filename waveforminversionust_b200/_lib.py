@@ -31,7 +31,7 @@ EXPORTED = (
     "wust_solver_create", "wust_solver_refactor", "wust_solver_destroy", "wust_solver_timings",
     "wust_solver_stencil", "wust_solver_block", "wust_solver_solve", "wust_solver_mass_apply",
     "wust_solver_oracle", "wust_solver_curvature", "wust_solver_gauss_newton_product", "wust_ncg_roi_gradient", "wust_ncg_direction",
-    "wust_ncg_dot", "wust_ncg_project", "wust_dtft", "wust_simulate", "wust_solver_stats", "wust_solver_factor_stats", "wust_solver_sweep_times",
+    "wust_ncg_dot", "wust_ncg_project", "wust_dtft", "wust_simulate", "wust_solver_stats", "wust_solver_factor_stats", "wust_solver_factor_info", "wust_solver_sweep_times",
     "wust_selftest_barrier_timeout",
 )
 
@@ -99,6 +99,7 @@ def load() -> C.CDLL:
     lib.wust_simulate.argtypes = [vp, i, i, d, d, d, i, vp, vp, i, vp, i, i, d, d, i, i, vp, vp]
     lib.wust_solver_stats.argtypes = [vp, pi, pd, pd, C.POINTER(C.c_longlong)]
     lib.wust_solver_factor_stats.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.wust_solver_factor_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.wust_solver_sweep_times.argtypes = [vp, pd, C.POINTER(C.c_longlong)]
     lib.wust_selftest_barrier_timeout.argtypes = [i, pi]
     for name in EXPORTED:

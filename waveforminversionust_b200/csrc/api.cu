@@ -176,6 +176,7 @@ struct wust_solver {
     int ns_head = 3;                  // pages inverted directly before the Newton-Schulz run (learned)
     NsGeom ns_g{};
     long long ns_stats[4] = {};       // GEMMs, X updates, Newton-Schulz pages, Gauss-Jordan pages
+    int ns_cluster = -1;              // last factorization: 1 cluster launches, 0 classic, -1 none
     float2 *stage_c = nullptr; size_t stage_c_cap = 0;
     double assembly_ms = 0, factor_ms = 0;
     int last_refine_iters = 0;
@@ -310,8 +311,9 @@ static void assemble_and_factor(wust_solver *s, const double *vel_in, const doub
         WUST_CUDA(cudaStreamSynchronize(st));
         check_assembly(astat0);
         for (long long &v : s->ns_stats) v = 0;
+        s->ns_cluster = -1;
         ns_factor(s->coefs64(), s->invT, s->ns_g, s->ns_scratch, s->fscratch, s->fscratch_bytes, st, s->ns_stats,
-                  &s->ns_head, s->max_ctas);
+                  &s->ns_head, s->max_ctas, &s->ns_cluster);
     } else {
         factor_launch(s->coefs64(), s->invT, s->fscratch, s->fscratch_bytes, st, 10.0, hstat, 0, -1, s->max_ctas);
     }
@@ -696,7 +698,7 @@ int wust_solver_create(wust_solver **out, const wust_solver_options *o, const do
             s->tc_part = dalloc<float>(s->tc_geom.part_bytes / sizeof(float));
             s->tc_sync = dalloc<unsigned>(s->tc_geom.sync_words);
             if (s->factor_method == WUST_FACTOR_DEFAULT) {
-                s->ns_g = ns_geom(ny, capped(ns_max_ctas()));
+                s->ns_g = ns_geom(ny, capped(ns_max_ctas()), s->max_ctas == 0);
                 if (s->ns_g.ks > 0) WUST_CUDA(cudaMalloc(&s->ns_scratch, s->ns_g.scratch_bytes));
             }
             s->tc_err = dalloc<int>(4);
@@ -1215,6 +1217,15 @@ int wust_solver_factor_stats(const wust_solver *s, long long out[4]) {
             out[0] = out[1] = out[2] = 0;
             out[3] = s->nx;
         }
+    });
+}
+
+int wust_solver_factor_info(const wust_solver *s, int *k_slices, int *cluster) {
+    return guarded([&] {
+        if (!s) fail(WUST_ERR_INVALID_INPUT, "null solver");
+        const bool ns = tensor_profile(s) && s->ns_scratch;
+        if (k_slices) *k_slices = ns ? s->ns_g.ks : 0;
+        if (cluster) *cluster = ns ? s->ns_cluster : -1;
     });
 }
 

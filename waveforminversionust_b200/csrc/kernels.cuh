@@ -117,9 +117,13 @@ void dtft_launch(const double *time_s, const double *freq, int nt, int nf, doubl
 // ---- nsfactor.cu (Newton-Schulz Schur inverses, TF32 tensor cores) ---------
 struct NsGeom {
     int n, mt, ntn, kc, ks, per;   // ks == 0: the grid does not fit; Gauss-Jordan only
+    int cluster;                   // 1: launched as clusters of the ks K slices of a tile
     size_t a_bytes, b_bytes, part_bytes, scratch_bytes;
 };
-NsGeom ns_geom(int ny, int max_ctas);
+// allow_cluster: the solver has the whole device (a solver confined to a
+// partition of the SMs runs the classic kernel: clusters need whole GPCs'
+// worth of free SMs, which partitions running side by side need not leave).
+NsGeom ns_geom(int ny, int max_ctas, bool allow_cluster);
 int ns_max_ctas();
 // All pages of invT: Newton-Schulz where the previous page is a good start,
 // the Gauss-Jordan kernel elsewhere (gj_scratch as for factor_launch).
@@ -128,8 +132,11 @@ int ns_max_ctas();
 // head_hint (in/out, may be null): the first page of the Newton-Schulz run
 // (at least 3); the pages before it go to one Gauss-Jordan launch.  Updated
 // from this factorization for the next one of the same solver.
+// cluster_used (out, may be null): 1 if the Newton-Schulz launches ran as
+// clusters, 0 if as the classic kernel; untouched without one.
 void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
-               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint, int max_ctas = 0);
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint, int max_ctas = 0,
+               int *cluster_used = nullptr);
 
 // ---- assemble.cu -----------------------------------------------------------
 struct AssemblyInput {

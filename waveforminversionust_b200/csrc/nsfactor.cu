@@ -39,6 +39,7 @@
 // barrier, the CTAs of a tile each sum one row slice in rank order and
 // write the epilogue (R in B layout, or X in A, B and fp32 layouts).
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -79,7 +80,61 @@ constexpr float kCubicLast = 0.04f;     // one cubic update, then accept
 constexpr float kFirstFail = 0.8f;      // X_{j-1} is no start for this column
 constexpr float kStallAccept = 0.05f;   // stalled at this level: finish with one update
 
-enum { NS_SITE_COPY = 21, NS_SITE_MMA = 22, NS_SITE_SYNC = 23 };
+enum { NS_SITE_COPY = 21, NS_SITE_MMA = 22, NS_SITE_SYNC = 23, NS_SITE_CLUSTER = 24 };
+
+// Cluster launch: the K slices of one tile form a thread-block cluster; each
+// CTA keeps its partial tile in its own shared memory (pitch kPartPitch
+// floats: 16-byte rows whose float4 stores from 8 consecutive TMEM lanes hit
+// distinct banks) at kPartOff, in the operand ring, which is idle from the
+// end of a GEMM to the grid barrier before the next one.
+constexpr int kPartPitch = NTN + 4;
+constexpr size_t kPartOff = 65536;
+static_assert(kPartOff + 128 * kPartPitch * sizeof(float) <= (size_t)kStages * kStageBytes, "partial tile in the ring");
+
+// Generic address of the same shared-memory location in cluster rank `rank`.
+template <typename T>
+__device__ __forceinline__ const T *peer_shared(const T *local, uint32_t rank) {
+    uint64_t out;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(local), "r"(rank));
+    return reinterpret_cast<const T *>(out);
+}
+
+// Hardware barrier of all threads of the cluster (unbounded: used only where
+// every thread of every CTA of the cluster arrives unconditionally).
+__device__ __forceinline__ void cluster_barrier_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Bounded barrier of the cluster's CTAs on a counter in rank 0's shared
+// memory (ctr: its shared::cluster address); false on an expired wait or a
+// reported error.
+__device__ __forceinline__ bool cluster_sync(uint32_t ctr, unsigned target, int *err, int *s_ok,
+                                             unsigned long long timeout_ns) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("fence.acq_rel.cluster;" ::: "memory");
+        asm volatile("red.release.cluster.shared::cluster.add.u32 [%0], %1;" ::"r"(ctr), "r"(1u) : "memory");
+        int ok = 1;
+        const unsigned long long t0 = global_timer_ns();
+        for (unsigned spin = 0;; ++spin) {
+            unsigned v;
+            asm volatile("ld.acquire.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(ctr) : "memory");
+            if ((int)(v - target) >= 0) break;
+            if ((spin & 15u) == 15u) {
+                if (*(volatile int *)err) { ok = 0; break; }
+                if (global_timer_ns() - t0 > timeout_ns) {
+                    atomicCAS(err, 0, NS_SITE_CLUSTER);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        asm volatile("fence.acq_rel.cluster;" ::: "memory");
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
 
 }  // namespace
 
@@ -110,7 +165,8 @@ struct NsParams {
     float2 *invT;            // [ny, ny, nx] column-major pages
     float2 *xf0, *xf1;       // X, fp32 complex, column-major n x n: an update reads one and writes the other
     float2 *xy;              // Y = X_k R_k of a cubic update, same layout
-    uint8_t *aT, *aX;        // A-packed T_j and X: [mt][kc] x 16 KB
+    uint8_t *aT;             // A-packed T_j: [mt][kc] x 16 KB
+    uint8_t *aX0, *aX1;      // A-packed X, same layout, with xf0 / xf1 (an update reads one and writes the other)
     uint8_t *bX, *bR;        // B-packed X and R:   [ntn][kc] x 14 KB
     float *part;             // [tile][ks][128][NTN]
     double *rn;              // [nblocks] per-CTA sums of |R|^2
@@ -162,6 +218,9 @@ __device__ __forceinline__ void put_x_packed(const NsParams &p, uint8_t *aX, uin
     *reinterpret_cast<float2 *>(bc + chunk_off(c % NTN, 2 * (r % kKRows))) = make_float2(xr, xi);
 }
 
+// CL: launched as clusters of the ks K slices of each tile (partials in
+// shared memory, read across the cluster); otherwise partials through L2.
+template <bool CL>
 __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *misc = smem + (size_t)kStages * kStageBytes;
@@ -172,6 +231,8 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     int *s_ok = reinterpret_cast<int *>(misc + 132);
     int *s_dec = reinterpret_cast<int *>(misc + 136);        // decision, r_k
     double *s_red = reinterpret_cast<double *>(misc + 192);  // one per warp
+    unsigned *s_cctr = reinterpret_cast<unsigned *>(misc + 384);   // cluster barrier counter (rank 0's is used)
+    float *spart = reinterpret_cast<float *>(smem + kPartOff);     // [128][kPartPitch] partial tile (CL)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mt = blockIdx.x, nb = blockIdx.y, ks = blockIdx.z;
@@ -196,6 +257,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(done, 1);
+        *s_cctr = 0u;
         tc::mbar_fence_init();
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, kTmemCols);
@@ -203,18 +265,28 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     __syncthreads();
     tc::fence_after();
     const uint32_t tmem = *tmem_slot;
+    // every CTA of the cluster has started (and zeroed its counter) before
+    // any shared memory of another is touched
+    if (CL) cluster_barrier_all();
+    const uint32_t cctr0 = CL ? (uint32_t)__cvta_generic_to_shared(s_cctr) : 0u;
+    uint32_t cctr = 0;
+    if (CL) asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(cctr) : "r"(cctr0), "r"(0u));
+    unsigned ctarget = 0;
 
     uint32_t u_issue = 0, u_cons = 0;    // ring counters (copy thread, thread 0)
     uint32_t n_gemm = 0;                 // GEMMs run (done-barrier phase)
     bool ok = true;
 
     // One GEMM C = Apack * Bpack^T over this CTA's K slice into TMEM, then
-    // the partial tile into L2.  Returns false on an expired wait.  The copy
-    // thread (kNsCopyTid) refills each stage as soon as the MMAs that read it
-    // have completed; thread 0 issues each chunk's MMAs as soon as its copies
-    // have landed.  Both count the chunks of every GEMM (u_issue, u_cons), so
-    // a stage's parity carries over from one GEMM to the next.
-    auto gemm = [&](const uint8_t *Apack, const uint8_t *Bpack) -> bool {
+    // the partial tile into L2 (or, CL, into this CTA's shared memory, and
+    // with `edges` the tile's first and last rows and columns also into L2,
+    // where the neighbouring tiles read their windows' halos).  Returns false
+    // on an expired wait.  The copy thread (kNsCopyTid) refills each stage as
+    // soon as the MMAs that read it have completed; thread 0 issues each
+    // chunk's MMAs as soon as its copies have landed.  Both count the chunks
+    // of every GEMM (u_issue, u_cons), so a stage's parity carries over from
+    // one GEMM to the next.
+    auto gemm = [&](const uint8_t *Apack, const uint8_t *Bpack, bool edges) -> bool {
         NSPROF(14);
         if (tid == kNsCopyTid) {
             const uint8_t *ab = Apack + ((size_t)mt * p.kc + c0) * tc::kAChunk;
@@ -263,6 +335,8 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         const int row = 32 * (warp & 3) + lane;
         const int cb0 = kPartCols * (warp >> 2);
         float *mypart = p.part + ((size_t)(tile * KS + ks) * 128 + row) * NTN + cb0;
+        float *myspart = spart + (size_t)row * kPartPitch + cb0;
+        const bool edge_row = (row & (kRows - 1)) == 0 || (row & (kRows - 1)) == kRows - 1;
 #pragma unroll
         for (int cb = 0; cb < kPartCols; cb += 8) {
             if (cb0 + cb >= NTN) break;                // warp-uniform
@@ -273,13 +347,36 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
 #pragma unroll
                 for (int q = 0; q < 8; ++q) t[q] = 0.f;
             }
-            __stcg(reinterpret_cast<float4 *>(mypart + cb), make_float4(t[0], t[1], t[2], t[3]));
-            __stcg(reinterpret_cast<float4 *>(mypart + cb + 4), make_float4(t[4], t[5], t[6], t[7]));
+            if (CL) {
+                *reinterpret_cast<float4 *>(myspart + cb) = make_float4(t[0], t[1], t[2], t[3]);
+                *reinterpret_cast<float4 *>(myspart + cb + 4) = make_float4(t[4], t[5], t[6], t[7]);
+                if (edges) {
+                    if (edge_row) {
+                        __stcg(reinterpret_cast<float4 *>(mypart + cb), make_float4(t[0], t[1], t[2], t[3]));
+                        __stcg(reinterpret_cast<float4 *>(mypart + cb + 4), make_float4(t[4], t[5], t[6], t[7]));
+                    } else {
+                        if (cb0 + cb == 0) __stcg(mypart + cb, t[0]);
+                        if (cb0 + cb + 8 == NTN) __stcg(mypart + cb + 7, t[7]);
+                    }
+                }
+            } else {
+                __stcg(reinterpret_cast<float4 *>(mypart + cb), make_float4(t[0], t[1], t[2], t[3]));
+                __stcg(reinterpret_cast<float4 *>(mypart + cb + 4), make_float4(t[4], t[5], t[6], t[7]));
+            }
         }
         tc::fence_before();
         NSPROF(3);
+        bool synced = true;
+        if (CL) {
+            ctarget += (unsigned)KS;
+            synced = cluster_sync(cctr, ctarget, p.err, s_ok, p.timeout_ns);
+            if (!edges) {
+                NSPROF(4);
+                return synced;
+            }
+        }
         epoch += (unsigned)nblocks;
-        const bool synced = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns);
+        synced = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns) && synced;
         NSPROF(4);
         return synced;
     };
@@ -297,6 +394,19 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
 #pragma unroll
         for (int m = 0; m < kEpi; ++m) v[m] = make_float2(0.f, 0.f);
         for (int q = 0; q < KS; ++q) {
+            if (CL) {                       // rank q of the cluster holds K slice q
+                const float *pq = peer_shared(spart, (uint32_t)q);
+#pragma unroll
+                for (int m = 0; m < kEpi; ++m) {
+                    const int it = tid + kNsThreads * m;
+                    if (it < n_items) {
+                        const int rl = rbeg + it / NTN, cl = it % NTN;
+                        v[m].x += pq[rl * kPartPitch + cl];
+                        v[m].y += pq[(rl + kRows) * kPartPitch + cl];
+                    }
+                }
+                continue;
+            }
             const float *pq = pt + (size_t)q * 128 * NTN;
 #pragma unroll
             for (int m = 0; m < kEpi; ++m) {
@@ -380,7 +490,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             const int r = idx % n, c = idx / n;
             const float2 v = X[(size_t)(r + 1) + (size_t)ny * (c + 1)];
             p.xf0[idx] = v;
-            put_x_packed(p, p.aX, p.bX, r, c, v);
+            put_x_packed(p, p.aX0, p.bX, r, c, v);
         }
         for (size_t idx = gtid; idx < (size_t)(p.j1 - p.j0) * 4 * ny; idx += gthreads) {
             const size_t page = p.j0 + idx / (4 * (size_t)ny);
@@ -502,9 +612,17 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 const float *pt = p.part + (size_t)((r / kRows) + p.mt * (c / NTN)) * KS * 128 * NTN;
                 const int rl = r % kRows, cl = c % NTN;
                 float vx = 0.f, vy = 0.f;
-                for (int q = 0; q < KS; ++q) {
-                    vx += __ldcg(pt + ((size_t)q * 128 + rl) * NTN + cl);
-                    vy += __ldcg(pt + ((size_t)q * 128 + rl + kRows) * NTN + cl);
+                if (CL && r / kRows == mt && c / NTN == nb) {     // this tile: the cluster's shared partials
+                    for (int q = 0; q < KS; ++q) {
+                        const float *pq = peer_shared(spart, (uint32_t)q);
+                        vx += pq[rl * kPartPitch + cl];
+                        vy += pq[(rl + kRows) * kPartPitch + cl];
+                    }
+                } else {                    // another tile's edge (CL: written to L2 by its last GEMM)
+                    for (int q = 0; q < KS; ++q) {
+                        vx += __ldcg(pt + ((size_t)q * 128 + rl) * NTN + cl);
+                        vy += __ldcg(pt + ((size_t)q * 128 + rl + kRows) * NTN + cl);
+                    }
                 }
                 float2 xo = Xold[(size_t)r + (size_t)n * c];
                 if (Yadd) {
@@ -541,7 +659,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         bool accepted = false;
         for (int k = 0; ok && !accepted && failed < 0; ++k) {
             // ---- R_k = I - T X_k (B layout) and its squared norm -----------
-            if (!(ok = gemm(p.aT, p.bX))) break;
+            if (!(ok = gemm(p.aT, p.bX, false))) break;
             ++n_gemms;
             double acc2 = 0.0;
             NSPROF(0);
@@ -624,7 +742,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 // ---- cubic last update: Y = X_k R_k (fp32 slice into xy, A
                 //      layout into aT, whose T_j is no longer read), then
                 //      X_{k+1} = X_k + Y + Y R_k ------------------------------
-                if (!(ok = gemm(p.aX, p.bR))) break;
+                if (!(ok = gemm(cur ? p.aX1 : p.aX0, p.bR, false))) break;
                 ++n_gemms;
                 NSPROF(0);
                 {
@@ -646,7 +764,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 epoch += (unsigned)nblocks;
                 if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
                 NSPROF(10);
-                if (!(ok = gemm(p.aT, p.bR))) break;
+                if (!(ok = gemm(p.aT, p.bR, j + 1 < p.j1))) break;
                 ++n_gemms;
                 ++n_updates;
                 NSPROF(0);
@@ -675,7 +793,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 __syncthreads();
                 write_cm(xnew, (size_t)n);
                 write_cm(page + ny + 1, (size_t)ny);
-                write_a(p.aX);
+                write_a(cur ? p.aX0 : p.aX1);
                 write_b(p.bX);
                 if (j + 1 < p.j1) {
                     __syncthreads();
@@ -691,7 +809,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 break;
             }
             // ---- X_{k+1} = X_k + X_k R_k ------------------------------------
-            if (!(ok = gemm(p.aX, p.bR))) break;
+            if (!(ok = gemm(cur ? p.aX1 : p.aX0, p.bR, dec == 1 && j + 1 < p.j1))) break;
             ++n_gemms;
             ++n_updates;
             const bool last = (dec == 1);
@@ -714,7 +832,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             __syncthreads();
             write_cm(xnew, (size_t)n);
             if (last) write_cm(page + ny + 1, (size_t)ny);
-            write_a(p.aX);
+            write_a(cur ? p.aX0 : p.aX1);
             write_b(p.bX);
             if (last && j + 1 < p.j1) {
                 // the next page's Schur complement from X_{k+1} (window
@@ -740,15 +858,46 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         p.status[3] = cols_done;
     }
     // drain: every issued copy was consumed and every MMA committed (the
-    // ring waits even after an expired wait), so TMEM can go
+    // ring waits even after an expired wait), so TMEM can go.  CL: no CTA
+    // leaves while another of its cluster may still read its shared memory
+    // (every wait above is bounded, so all of them get here)
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
     if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+    if (CL) cluster_barrier_all();
 }
 
 // ---------------------------------------------------------------------------
-NsGeom ns_geom(int ny, int max_ctas) {
+// Cluster launches unless WUST_NS_CLUSTER=0 (the classic path, partials
+// through L2, for comparison).
+static bool ns_cluster_enabled() {
+    const char *e = std::getenv("WUST_NS_CLUSTER");
+    return !(e && e[0] == '0');
+}
+
+// How many clusters of ks CTAs (one per SM) the device holds at once.
+static int ns_max_clusters(int mt, int ntn, int ks) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(mt, ntn, ks);
+    cfg.blockDim = dim3(kNsThreads);
+    cfg.dynamicSmemBytes = kNsSmem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 1;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = ks;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, ns_factor_kernel<true>, &cfg) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+NsGeom ns_geom(int ny, int max_ctas, bool allow_cluster) {
     NsGeom g{};
     g.n = ny - 2;
     g.mt = ceil_div(g.n, kRows);
@@ -758,11 +907,23 @@ NsGeom ns_geom(int ny, int max_ctas) {
     g.ks = std::max(1, std::min(max_ctas / std::max(tiles, 1), 8));
     g.ks = std::min(g.ks, g.kc);
     if (g.ks < 3) g.ks = 0;                   // outside the epilogue bound: Gauss-Jordan only
+    // the largest K split whose clusters all fit at once (a cluster's CTAs
+    // share one GPC, so fewer clusters of 8 fit than 148 / 8)
+    g.cluster = 0;
+    if (g.ks > 0 && allow_cluster && ns_cluster_enabled()) {
+        for (int ks = g.ks; ks >= 3; --ks) {
+            if (ns_max_clusters(g.mt, g.ntn, ks) >= tiles) {
+                g.ks = ks;
+                g.cluster = 1;
+                break;
+            }
+        }
+    }
     g.per = g.ks > 0 ? ceil_div(g.kc, g.ks) : 0;
     g.a_bytes = (size_t)g.mt * g.kc * tc::kAChunk;
     g.b_bytes = (size_t)g.ntn * g.kc * kBChunkNs;
     g.part_bytes = (size_t)tiles * std::max(g.ks, 1) * 128 * NTN * sizeof(float);
-    g.scratch_bytes = 2 * g.a_bytes + 2 * g.b_bytes + g.part_bytes + 3 * (size_t)g.n * g.n * sizeof(float2) +
+    g.scratch_bytes = 3 * g.a_bytes + 2 * g.b_bytes + g.part_bytes + 3 * (size_t)g.n * g.n * sizeof(float2) +
                       (size_t)max_ctas * sizeof(double) + 256;
     return g;
 }
@@ -770,24 +931,27 @@ NsGeom ns_geom(int ny, int max_ctas) {
 int ns_max_ctas() {
     int dev = 0, sms = 0, per_sm = 0;
     WUST_CUDA(cudaGetDevice(&dev));
-    // the attribute lives in the current device's context (set every time: a
+    // the attributes live in the current device's context (set every time: a
     // caller may switch devices or reset one between calls)
-    WUST_CUDA(cudaFuncSetAttribute(ns_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNsSmem));
+    WUST_CUDA(cudaFuncSetAttribute(ns_factor_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNsSmem));
+    WUST_CUDA(cudaFuncSetAttribute(ns_factor_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNsSmem));
     WUST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    WUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ns_factor_kernel, kNsThreads, kNsSmem));
+    WUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ns_factor_kernel<false>, kNsThreads, kNsSmem));
     return sms * per_sm;
 }
 
 // Launch the Newton-Schulz pages [j0, j1); returns the first page it gave
-// back (or -1) and adds its GEMM/update counts to stats.
+// back (or -1) and adds its GEMM/update counts to stats; *cluster_used
+// (nullable) says whether it ran as clusters.
 static int ns_launch(const Coefs<float2> &co, float2 *invT, const NsGeom &g, uint8_t *scratch, int j0, int j1,
-                     cudaStream_t st, long long *stats) {
+                     cudaStream_t st, long long *stats, int *cluster_used) {
     NsParams p;
     p.co = co;
     p.invT = invT;
     uint8_t *q = scratch;
     p.aT = q; q += g.a_bytes;
-    p.aX = q; q += g.a_bytes;
+    p.aX0 = q; q += g.a_bytes;
+    p.aX1 = q; q += g.a_bytes;
     p.bX = q; q += g.b_bytes;
     p.bR = q; q += g.b_bytes;
     p.part = reinterpret_cast<float *>(q); q += g.part_bytes;
@@ -812,11 +976,36 @@ static int ns_launch(const Coefs<float2> &co, float2 *invT, const NsGeom &g, uin
     p.max_iter = 8;
     p.timeout_ns = 2000000000ull;
     // packed operands: padding entries must be zero (never written later)
-    WUST_CUDA(cudaMemsetAsync(scratch, 0, 2 * g.a_bytes + 2 * g.b_bytes, st));
+    WUST_CUDA(cudaMemsetAsync(scratch, 0, 3 * g.a_bytes + 2 * g.b_bytes, st));
     WUST_CUDA(cudaMemsetAsync(tail, 0, 8 * sizeof(int), st));
-    void *args[] = {&p};
-    WUST_CUDA(cudaLaunchCooperativeKernel((void *)ns_factor_kernel, dim3(g.mt, g.ntn, g.ks), dim3(kNsThreads), args,
-                                          kNsSmem, st));
+    bool launched = false;
+    if (g.cluster) {
+        // cooperative (every CTA resident at once) and clustered (the K
+        // slices of a tile in one cluster); a runtime that refuses the pair
+        // gets the classic kernel on the same geometry
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(g.mt, g.ntn, g.ks);
+        cfg.blockDim = dim3(kNsThreads);
+        cfg.dynamicSmemBytes = kNsSmem;
+        cfg.stream = st;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 1;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = g.ks;
+        at[1].id = cudaLaunchAttributeCooperative;
+        at[1].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 2;
+        if (cudaLaunchKernelEx(&cfg, ns_factor_kernel<true>, p) == cudaSuccess) launched = true;
+        else (void)cudaGetLastError();
+    }
+    if (cluster_used) *cluster_used = launched ? 1 : 0;
+    if (!launched) {
+        void *args[] = {&p};
+        WUST_CUDA(cudaLaunchCooperativeKernel((void *)ns_factor_kernel<false>, dim3(g.mt, g.ntn, g.ks),
+                                              dim3(kNsThreads), args, kNsSmem, st));
+    }
     ++g_kernel_launches;
     WUST_LAUNCH_CHECK();
     int h[6];
@@ -863,7 +1052,8 @@ __global__ void identity_page_kernel(Coefs<float2> co, float2 *invT, int j, int 
 }
 
 void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_scratch, void *gj_scratch,
-               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint, int max_ctas) {
+               size_t gj_scratch_bytes, cudaStream_t st, long long *stats, int *head_hint, int max_ctas,
+               int *cluster_used) {
     const int nx = co.nx;
     int hstat[3];
     auto gj = [&](int a, int b) {
@@ -908,7 +1098,7 @@ void ns_factor(const Coefs<float2> &co, float2 *invT, const NsGeom &g, void *ns_
             j = nx - 1;
             break;
         }
-        const int bad = ns_launch(co, invT, g, (uint8_t *)ns_scratch, j, nx - 1, st, stats);
+        const int bad = ns_launch(co, invT, g, (uint8_t *)ns_scratch, j, nx - 1, st, stats, cluster_used);
         leading = leading && bad == j;
         if (leading) learned = bad + 1;
         if (bad < 0) {

@@ -256,6 +256,14 @@ class HelmholtzSolver:
         check(self._lib.wust_solver_factor_stats(self._h, out))
         return {"gemms": out[0], "updates": out[1], "newton_schulz_pages": out[2], "gauss_jordan_pages": out[3]}
 
+    def factor_info(self):
+        """K split of the Newton-Schulz GEMM tiles and whether the last
+        factorization ran them as thread-block clusters (1), as separate CTAs
+        (0) or not at all (-1)."""
+        ks, cl = C.c_int(), C.c_int()
+        check(self._lib.wust_solver_factor_info(self._h, C.byref(ks), C.byref(cl)))
+        return {"k_slices": ks.value, "cluster": cl.value}
+
 
 def decompBlockLU(Ld, Ll, Lu, Dd, Dl, Du, Ud, Ul, Uu, stream=None, timings=False):
     """Drop-in for the decompBlockLU MEX (decompBlockLU.cu:173-396) on CUDA tensors.
