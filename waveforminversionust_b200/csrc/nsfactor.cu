@@ -56,12 +56,15 @@ namespace {
 constexpr int NTN = 112;                           // MMA N: complex columns per tile
 constexpr int kRows = 64;                          // complex rows per M tile
 constexpr int kKRows = 16;                         // complex K rows per chunk
-constexpr int kStages = 7;
+constexpr int kStages = 5;
 constexpr int kNsThreads = 512;
 constexpr int kPartCols = (NTN / (kNsThreads / 128) + 7) / 8 * 8;   // TMEM columns per warp of the partial tile
 constexpr int kBChunkNs = NTN * tc::kChunkBytes;   // 14 KB
 constexpr int kStageBytes = tc::kAChunk + kBChunkNs;
-constexpr size_t kNsSmem = (size_t)kStages * kStageBytes + 512;
+constexpr int kSP = NTN + 1;                       // pitch (float2) of a staged slice row
+constexpr int kSliceRows = ((kRows + 2) / 3 + 1) & ~1;   // rows of the largest slice (ks >= 3)
+// ring, barriers and scalars, then this CTA's resident X and Y slices
+constexpr size_t kNsSmem = (size_t)kStages * kStageBytes + 512 + 2 * (size_t)kSliceRows * kSP * sizeof(float2);
 static_assert(kNsSmem <= 232448, "shared memory of one CTA");
 constexpr int kTmemCols = 128;
 constexpr int kNsCopyTid = 96;                     // the ring's copy thread (warp 3, lane 0)
@@ -233,6 +236,11 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     double *s_red = reinterpret_cast<double *>(misc + 192);  // one per warp
     unsigned *s_cctr = reinterpret_cast<unsigned *>(misc + 384);   // cluster barrier counter (rank 0's is used)
     float *spart = reinterpret_cast<float *>(smem + kPartOff);     // [128][kPartPitch] partial tile (CL)
+    // this CTA's slice of the current X and of a cubic update's Y, resident
+    // across the GEMMs (outside the ring); global memory keeps only the
+    // values other CTAs' windows read
+    float2 *sxk = reinterpret_cast<float2 *>(misc + 512);          // [kSliceRows][kSP]
+    float2 *syk = sxk + (size_t)kSliceRows * kSP;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mt = blockIdx.x, nb = blockIdx.y, ks = blockIdx.z;
@@ -423,20 +431,20 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     // Staging of this CTA's slice (rows rbeg..rend-1 of the M tile, all NTN
     // columns) in the operand ring, which is idle between GEMMs; from there
     // every packed layout is written in whole 16-byte units.
-    constexpr int SP = NTN + 1;                                  // staged row pitch (float2)
+    constexpr int SP = kSP;                                      // staged row pitch (float2)
     float2 *sx = reinterpret_cast<float2 *>(smem);               // [rows_per][SP]
     float2 *xw = reinterpret_cast<float2 *>(smem + 32768);       // Schur window [rows_per + 2][SP + 2]
     const int nr = rend - rbeg;
     const int grow0 = mt * kRows + rbeg;                         // global row of slice row 0
     const int gcol0 = nb * NTN;
     // A layout (rows i_s = r % 64 and r % 64 + 64, K units of two columns)
-    auto write_a = [&](uint8_t *Apack) {
+    auto write_a = [&](uint8_t *Apack, const float2 *src) {
         for (int u = tid; u < nr * (NTN / 2); u += kNsThreads) {
             const int rl = u % nr, cp = u / nr;
             const int r = grow0 + rl, c = gcol0 + 2 * cp;
             if (r >= n || c >= n) continue;
-            const float2 y0 = sx[rl * SP + 2 * cp];
-            const float2 y1 = c + 1 < n ? sx[rl * SP + 2 * cp + 1] : make_float2(0.f, 0.f);
+            const float2 y0 = src[rl * SP + 2 * cp];
+            const float2 y1 = c + 1 < n ? src[rl * SP + 2 * cp + 1] : make_float2(0.f, 0.f);
             uint8_t *ac = Apack + ((size_t)mt * p.kc + c / kKRows) * tc::kAChunk;
             const int ke = 2 * (c % kKRows);
             *reinterpret_cast<float4 *>(ac + chunk_off(r % kRows, ke)) =
@@ -446,39 +454,38 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         }
     };
     // B layout (column cl, K units of two rows)
-    auto write_b = [&](uint8_t *Bpack) {
+    auto write_b = [&](uint8_t *Bpack, const float2 *src) {
         for (int u = tid; u < (nr / 2) * NTN; u += kNsThreads) {
             const int cl = u % NTN, rp = u / NTN;
             const int r = grow0 + 2 * rp, c = gcol0 + cl;
             if (r >= n || c >= n) continue;
-            const float2 z0 = sx[(2 * rp) * SP + cl];
-            const float2 z1 = r + 1 < n ? sx[(2 * rp + 1) * SP + cl] : make_float2(0.f, 0.f);
+            const float2 z0 = src[(2 * rp) * SP + cl];
+            const float2 z1 = r + 1 < n ? src[(2 * rp + 1) * SP + cl] : make_float2(0.f, 0.f);
             uint8_t *bc = Bpack + ((size_t)nb * p.kc + r / kKRows) * kBChunkNs;
             *reinterpret_cast<float4 *>(bc + chunk_off(cl, 2 * (r % kKRows))) =
                 make_float4(to_tf32(z0.x), to_tf32(z0.y), to_tf32(z1.x), to_tf32(z1.y));
         }
     };
     // column-major copy (leading dimension ld, element (r, c) at base[r + ld c])
-    auto write_cm = [&](float2 *base, size_t ld) {
+    auto write_cm = [&](float2 *base, size_t ld, const float2 *src) {
         for (int u = tid; u < nr * NTN; u += kNsThreads) {
             const int rl = u % nr, cl = u / nr;
             const int r = grow0 + rl, c = gcol0 + cl;
-            if (r < n && c < n) base[(size_t)r + ld * c] = sx[rl * SP + cl];
+            if (r < n && c < n) base[(size_t)r + ld * c] = src[rl * SP + cl];
         }
     };
-    auto read_cm = [&](const float2 *base, size_t ld) {
-        float2 v[kEpi];                      // all loads first, then the stores
-#pragma unroll
-        for (int m = 0; m < kEpi; ++m) {
-            const int u = tid + kNsThreads * m;
-            const int rl = u % max(nr, 1), cl = u / max(nr, 1);
+    // the values of the slice that other CTAs' windows read (its first and
+    // last rows, the tile's first and last columns) into an n x n
+    // column-major array
+    auto write_edges = [&](float2 *base, const float2 *src) {
+        for (int u = tid; u < 2 * NTN + 2 * nr; u += kNsThreads) {
+            int rl, cl;
+            if (u < NTN) { rl = 0; cl = u; }
+            else if (u < 2 * NTN) { rl = nr - 1; cl = u - NTN; }
+            else if (u < 2 * NTN + nr) { rl = u - 2 * NTN; cl = 0; }
+            else { rl = u - 2 * NTN - nr; cl = NTN - 1; }
             const int r = grow0 + rl, c = gcol0 + cl;
-            v[m] = (u < nr * NTN && r < n && c < n) ? base[(size_t)r + ld * c] : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int m = 0; m < kEpi; ++m) {
-            const int u = tid + kNsThreads * m;
-            if (u < nr * NTN) sx[(u % nr) * SP + u / nr] = v[m];
+            if (r < n && c < n) base[(size_t)r + (size_t)n * c] = src[rl * SP + cl];
         }
     };
 
@@ -501,6 +508,11 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                              : which == 2 ? (size_t)k
                                           : (size_t)k + (size_t)ny * (ny - 1);
             p.invT[page * page_sz + off] = make_float2(0.f, 0.f);
+        }
+        for (int u = tid; u < nr * NTN; u += kNsThreads) {
+            const int rl = u / NTN, cl = u % NTN;
+            const int r = grow0 + rl, c = gcol0 + cl;
+            sxk[rl * SP + cl] = r < n && c < n ? X[(size_t)(r + 1) + (size_t)ny * (c + 1)] : make_float2(0.f, 0.f);
         }
         epoch += (unsigned)nblocks;
         ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns);
@@ -573,28 +585,32 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             sx[rl * SP + cl] = v;
         }
         __syncthreads();
-        write_a(p.aT);
+        write_a(p.aT, sx);
     };
     // window of an X held whole in global memory (all loads of a thread in flight)
+    // window of the current X: the slice from sxk, the halo ring from the
+    // edges its owners wrote to X (global)
     auto window_from = [&](const float2 *X) {
-        constexpr int kWin = ((kRows / 3 + 4) * (NTN + 2) + kNsThreads - 1) / kNsThreads;
-        float2 v[kWin];
-#pragma unroll
-        for (int m = 0; m < kWin; ++m) {
-            const int u = tid + kNsThreads * m;
-            const int rw = u % wr, cwi = u / wr;
-            const int r = grow0 - 1 + rw, c = gcol0 - 1 + cwi;
-            v[m] = (u < wr * wc && r >= 0 && r < n && c >= 0 && c < n) ? X[(size_t)r + (size_t)n * c]
-                                                                        : make_float2(0.f, 0.f);
+        const int n_halo = 2 * wc + 2 * nr;
+        if (tid < n_halo) {
+            const int h = tid;
+            int hrw, hcw;
+            if (h < wc) { hrw = 0; hcw = h; }
+            else if (h < 2 * wc) { hrw = nr + 1; hcw = h - wc; }
+            else if (h < 2 * wc + nr) { hrw = 1 + (h - 2 * wc); hcw = 0; }
+            else { hrw = 1 + (h - 2 * wc - nr); hcw = NTN + 1; }
+            const int r = grow0 - 1 + hrw, c = gcol0 - 1 + hcw;
+            xw[hrw * (SP + 2) + hcw] =
+                r >= 0 && r < n && c >= 0 && c < n ? X[(size_t)r + (size_t)n * c] : make_float2(0.f, 0.f);
         }
-#pragma unroll
-        for (int m = 0; m < kWin; ++m) {
-            const int u = tid + kNsThreads * m;
-            if (u < wr * wc) xw[(u % wr) * (SP + 2) + u / wr] = v[m];
+        for (int u = tid; u < nr * NTN; u += kNsThreads) {
+            const int rl = u / NTN, cl = u % NTN;
+            const bool in = grow0 + rl < n && gcol0 + cl < n;
+            xw[(rl + 1) * (SP + 2) + cl + 1] = in ? sxk[rl * SP + cl] : make_float2(0.f, 0.f);
         }
     };
     // window of X_{k+1} = X_k + (X_k R_k) right after an update: the slice is
-    // in sx; each halo value is its owner's sum, formed here the same way
+    // in sxk; each halo value is its owner's sum, formed here the same way
     // (X_k from Xold plus the split-K partials of the owner's tile, in rank
     // order), so no barrier is needed before the next Schur complement
     auto window_after_update = [&](const float2 *Xold, const float2 *Yadd) {
@@ -635,7 +651,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         for (int u = tid; u < nr * NTN; u += kNsThreads) {
             const int rl = u / NTN, cl = u % NTN;
             const bool in = grow0 + rl < n && gcol0 + cl < n;
-            xw[(rl + 1) * (SP + 2) + cl + 1] = in ? sx[rl * SP + cl] : make_float2(0.f, 0.f);
+            xw[(rl + 1) * (SP + 2) + cl + 1] = in ? sxk[rl * SP + cl] : make_float2(0.f, 0.f);
         }
         if (tid < n_halo) xw[hrw * (SP + 2) + hcw] = hv;
     };
@@ -680,7 +696,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 sx[rl * SP + cl] = rv;
             }
             __syncthreads();
-            write_b(p.bR);
+            write_b(p.bR, sx);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc2 += __shfl_xor_sync(0xffffffffu, acc2, o);
             if (lane == 0) s_red[warp] = acc2;
@@ -731,17 +747,14 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 // X_k stays: copy it into page j.  No barrier: nothing of the
                 // next page's Schur complement writes what another CTA reads
                 float2 *page = p.invT + (size_t)j * page_sz;
-                read_cm(cur ? p.xf1 : p.xf0, (size_t)n);
-                __syncthreads();
-                write_cm(page + ny + 1, (size_t)ny);
-                __syncthreads();
+                write_cm(page + ny + 1, (size_t)ny, sxk);
                 accepted = true;
                 break;
             }
             if (dec == 4) {
-                // ---- cubic last update: Y = X_k R_k (fp32 slice into xy, A
-                //      layout into aT, whose T_j is no longer read), then
-                //      X_{k+1} = X_k + Y + Y R_k ------------------------------
+                // ---- cubic last update: Y = X_k R_k (the slice into syk, its
+                //      edges into xy, A layout into aT, whose T_j is no longer
+                //      read), then X_{k+1} = X_k + Y + Y R_k -------------------
                 if (!(ok = gemm(cur ? p.aX1 : p.aX0, p.bR, false))) break;
                 ++n_gemms;
                 NSPROF(0);
@@ -754,12 +767,12 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                         if (it >= n_items) break;
                         const int rl = it / NTN, cl = it % NTN;
                         const bool in = grow0 + rl < n && gcol0 + cl < n;
-                        sx[rl * SP + cl] = in ? pv[m] : make_float2(0.f, 0.f);
+                        syk[rl * SP + cl] = in ? pv[m] : make_float2(0.f, 0.f);
                     }
                 }
                 __syncthreads();
-                write_cm(p.xy, (size_t)n);
-                write_a(p.aT);
+                write_edges(p.xy, syk);
+                write_a(p.aT, syk);
                 NSPROF(9);
                 epoch += (unsigned)nblocks;
                 if (!(ok = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns))) break;
@@ -771,35 +784,30 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 float2 *page = p.invT + (size_t)j * page_sz;
                 const float2 *xold = cur ? p.xf1 : p.xf0;
                 float2 *xnew = cur ? p.xf0 : p.xf1;
-                read_cm(xold, (size_t)n);              // X_k of the slice
-                float2 pvx[kEpi], yv[kEpi];
+                float2 pvx[kEpi];
                 tile_values(pvx);
 #pragma unroll
-                for (int m = 0; m < kEpi; ++m) {
-                    const int it = tid + kNsThreads * m;
-                    const int r = grow0 + it / NTN, c = gcol0 + it % NTN;
-                    yv[m] = (it < n_items && r < n && c < n) ? __ldcg(p.xy + (size_t)r + (size_t)n * c)
-                                                              : make_float2(0.f, 0.f);
-                }
-                __syncthreads();
-#pragma unroll
-                for (int m = 0; m < kEpi; ++m) {
+                for (int m = 0; m < kEpi; ++m) {     // X_{k+1} = X_k + Y + Y R_k, in place
                     const int it = tid + kNsThreads * m;
                     if (it >= n_items) break;
                     const int rl = it / NTN, cl = it % NTN;
-                    float2 &x = sx[rl * SP + cl];
-                    x = make_float2(x.x + yv[m].x + pvx[m].x, x.y + yv[m].y + pvx[m].y);
+                    float2 &x = sxk[rl * SP + cl];
+                    const float2 y = syk[rl * SP + cl];
+                    x = make_float2(x.x + y.x + pvx[m].x, x.y + y.y + pvx[m].y);
                 }
                 __syncthreads();
-                write_cm(xnew, (size_t)n);
-                write_cm(page + ny + 1, (size_t)ny);
-                write_a(cur ? p.aX0 : p.aX1);
-                write_b(p.bX);
+                NSPROF(12);
+                write_edges(xnew, sxk);
+                write_cm(page + ny + 1, (size_t)ny, sxk);
+                write_a(cur ? p.aX0 : p.aX1, sxk);
+                write_b(p.bX, sxk);
+                NSPROF(13);
                 if (j + 1 < p.j1) {
                     __syncthreads();
                     build_T(j + 1, [&] { window_after_update(xold, p.xy); });
                     t_ready = true;
                 }
+                NSPROF(15);
                 cur ^= 1;
                 NSPROF(9);
                 epoch += (unsigned)nblocks;
@@ -817,23 +825,23 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
             float2 *page = p.invT + (size_t)j * page_sz;
             const float2 *xold = cur ? p.xf1 : p.xf0;
             float2 *xnew = cur ? p.xf0 : p.xf1;
-            read_cm(xold, (size_t)n);                  // X_k of the slice
             float2 pvx[kEpi];
             tile_values(pvx);
-            __syncthreads();
 #pragma unroll
-            for (int m = 0; m < kEpi; ++m) {
+            for (int m = 0; m < kEpi; ++m) {         // X_{k+1} = X_k + X_k R_k, in place
                 const int it = tid + kNsThreads * m;
                 if (it >= n_items) break;
                 const int rl = it / NTN, cl = it % NTN;
-                float2 &x = sx[rl * SP + cl];
+                float2 &x = sxk[rl * SP + cl];
                 x = make_float2(x.x + pvx[m].x, x.y + pvx[m].y);
             }
             __syncthreads();
-            write_cm(xnew, (size_t)n);
-            if (last) write_cm(page + ny + 1, (size_t)ny);
-            write_a(cur ? p.aX0 : p.aX1);
-            write_b(p.bX);
+            NSPROF(12);
+            write_edges(xnew, sxk);
+            if (last) write_cm(page + ny + 1, (size_t)ny, sxk);
+            write_a(cur ? p.aX0 : p.aX1, sxk);
+            write_b(p.bX, sxk);
+            NSPROF(13);
             if (last && j + 1 < p.j1) {
                 // the next page's Schur complement from X_{k+1} (window
                 // formed without a barrier), ready at this update's barrier
@@ -841,6 +849,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
                 build_T(j + 1, [&] { window_after_update(xold, nullptr); });
                 t_ready = true;
             }
+            NSPROF(15);
             cur ^= 1;
             NSPROF(9);
             epoch += (unsigned)nblocks;
