@@ -375,13 +375,14 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
         tc::fence_before();
         NSPROF(3);
         bool synced = true;
-        if (CL) {
+        // CL: the cluster's barrier publishes the shared partials; a GEMM
+        // with edges needs the grid barrier, whose gpu-scope release and
+        // acquire cover the cluster's shared memory too
+        if (CL && !edges) {
             ctarget += (unsigned)KS;
             synced = cluster_sync(cctr, ctarget, p.err, s_ok, p.timeout_ns);
-            if (!edges) {
-                NSPROF(4);
-                return synced;
-            }
+            NSPROF(4);
+            return synced;
         }
         epoch += (unsigned)nblocks;
         synced = ns_sync(p.ctr, epoch, p.err, s_ok, p.timeout_ns) && synced;

@@ -447,8 +447,8 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                 if (s < N && gs < p.s_end) {
                     if (old_u) {
                         const float2 *uc = p.u + plane * gs + (size_t)ny * j;
-                        if (v0) o[q][0] = __ldcg(uc + y0);
-                        if (v1) o[q][1] = __ldcg(uc + y0 + 1);
+                        if (v0) o[q][0] = __ldcs(uc + y0);
+                        if (v1) o[q][1] = __ldcs(uc + y0 + 1);
                     } else if (kind == K_BOUND) {
                         const float *ore = oldp + (size_t)(so + s) * ny, *oim = oldp + (size_t)(kCkMaxN + so + s) * ny;
                         if (v0) o[q][0] = f2(__ldcg(ore + y0), __ldcg(oim + y0));
@@ -469,10 +469,10 @@ __global__ void __launch_bounds__(kCkThreads, 1) tc_chunk_kernel(const __grid_co
                     *cp4 = cv;
                 }
                 if (gs >= p.s_end) continue;
-                if (wu) {
+                if (wu) {                 // u streams through L2 (evict first), as the old column it replaces
                     float2 *uc = p.u + plane * gs + (size_t)ny * j;
-                    if (v0) uc[y0] = f2(cv.x, cv.y);
-                    if (v1) uc[y0 + 1] = f2(cv.z, cv.w);
+                    if (v0) __stcs(uc + y0, f2(cv.x, cv.y));
+                    if (v1) __stcs(uc + y0 + 1, f2(cv.z, cv.w));
                 }
                 if (lane == 0) __stcg(my_edges + s, f2(cv.x, cv.y));
                 if (lane == 31 && v1) __stcg(my_edges + kCkMaxN + s, f2(cv.z, cv.w));
