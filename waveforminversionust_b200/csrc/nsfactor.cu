@@ -39,6 +39,7 @@
 // barrier, the CTAs of a tile each sum one row slice in rank order and
 // write the epilogue (R in B layout, or X in A, B and fp32 layouts).
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <vector>
 
@@ -83,7 +84,7 @@ constexpr float kCubicLast = 0.04f;     // one cubic update, then accept
 constexpr float kFirstFail = 0.8f;      // X_{j-1} is no start for this column
 constexpr float kStallAccept = 0.05f;   // stalled at this level: finish with one update
 
-enum { NS_SITE_COPY = 21, NS_SITE_MMA = 22, NS_SITE_SYNC = 23, NS_SITE_CLUSTER = 24 };
+enum { NS_SITE_COPY = 21, NS_SITE_MMA = 22, NS_SITE_SYNC = 23, NS_SITE_CLUSTER = 24, NS_SITE_SHAPE = 25 };
 
 // Cluster launch: the K slices of one tile form a thread-block cluster; each
 // CTA keeps its partial tile in its own shared memory (pitch kPartPitch
@@ -284,6 +285,19 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
     uint32_t u_issue = 0, u_cons = 0;    // ring counters (copy thread, thread 0)
     uint32_t n_gemm = 0;                 // GEMMs run (done-barrier phase)
     bool ok = true;
+    if (CL) {
+        // the K slices of this tile must be this cluster, in rank order;
+        // launched in any other shape (the same in every CTA), no CTA does
+        // any work or touches another's shared memory, and the host reruns
+        // the pages with the classic kernel
+        uint32_t ncta, rank;
+        asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
+        asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+        if (ncta != (uint32_t)KS || rank != (uint32_t)ks) {
+            if (tid == 0) atomicCAS(p.err, 0, NS_SITE_SHAPE);
+            ok = false;
+        }
+    }
 
     // One GEMM C = Apack * Bpack^T over this CTA's K slice into TMEM, then
     // the partial tile into L2 (or, CL, into this CTA's shared memory, and
@@ -492,7 +506,7 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
 
     // ---- start: X = invT_{j0-1} into the fp32 and packed copies; zero the
     //      borders of the pages this launch writes ----------------------------
-    {
+    if (ok) {
         const float2 *X = p.invT + (size_t)(p.j0 - 1) * page_sz;
         for (int idx = gtid; idx < n * n; idx += gthreads) {
             const int r = idx % n, c = idx / n;
@@ -880,7 +894,9 @@ __global__ void __launch_bounds__(kNsThreads, 1) ns_factor_kernel(NsParams p) {
 
 // ---------------------------------------------------------------------------
 // Cluster launches unless WUST_NS_CLUSTER=0 (the classic path, partials
-// through L2, for comparison).
+// through L2, for comparison), or once a launch ran without its clusters.
+static std::atomic<bool> g_ns_cluster_off{false};
+
 static bool ns_cluster_enabled() {
     const char *e = std::getenv("WUST_NS_CLUSTER");
     return !(e && e[0] == '0');
@@ -988,8 +1004,13 @@ static int ns_launch(const Coefs<float2> &co, float2 *invT, const NsGeom &g, uin
     // packed operands: padding entries must be zero (never written later)
     WUST_CUDA(cudaMemsetAsync(scratch, 0, 3 * g.a_bytes + 2 * g.b_bytes, st));
     WUST_CUDA(cudaMemsetAsync(tail, 0, 8 * sizeof(int), st));
+    int h[6];
+    auto read_tail = [&] {
+        WUST_CUDA(cudaMemcpyAsync(h, tail, sizeof(h), cudaMemcpyDeviceToHost, st));
+        WUST_CUDA(cudaStreamSynchronize(st));
+    };
     bool launched = false;
-    if (g.cluster) {
+    if (g.cluster && !g_ns_cluster_off.load()) {
         // cooperative (every CTA resident at once) and clustered (the K
         // slices of a tile in one cluster); a runtime that refuses the pair
         // gets the classic kernel on the same geometry
@@ -1007,20 +1028,31 @@ static int ns_launch(const Coefs<float2> &co, float2 *invT, const NsGeom &g, uin
         at[1].val.cooperative = 1;
         cfg.attrs = at;
         cfg.numAttrs = 2;
-        if (cudaLaunchKernelEx(&cfg, ns_factor_kernel<true>, p) == cudaSuccess) launched = true;
-        else (void)cudaGetLastError();
+        if (cudaLaunchKernelEx(&cfg, ns_factor_kernel<true>, p) == cudaSuccess) {
+            launched = true;
+            ++g_kernel_launches;
+            WUST_LAUNCH_CHECK();
+            read_tail();
+            if (h[1] == NS_SITE_SHAPE) {
+                // the launch did not get its clusters (the kernel did nothing):
+                // the classic kernel from here on in this process
+                g_ns_cluster_off.store(true);
+                launched = false;
+                WUST_CUDA(cudaMemsetAsync(tail, 0, 8 * sizeof(int), st));
+            }
+        } else {
+            (void)cudaGetLastError();
+        }
     }
     if (cluster_used) *cluster_used = launched ? 1 : 0;
     if (!launched) {
         void *args[] = {&p};
         WUST_CUDA(cudaLaunchCooperativeKernel((void *)ns_factor_kernel<false>, dim3(g.mt, g.ntn, g.ks),
                                               dim3(kNsThreads), args, kNsSmem, st));
+        ++g_kernel_launches;
+        WUST_LAUNCH_CHECK();
+        read_tail();
     }
-    ++g_kernel_launches;
-    WUST_LAUNCH_CHECK();
-    int h[6];
-    WUST_CUDA(cudaMemcpyAsync(h, tail, sizeof(h), cudaMemcpyDeviceToHost, st));
-    WUST_CUDA(cudaStreamSynchronize(st));
     if (h[1]) fail(WUST_ERR_DEVICE_TIMEOUT, "Newton-Schulz factorization: device wait expired (site %d)", h[1]);
     if (stats) {
         stats[0] += h[3];
