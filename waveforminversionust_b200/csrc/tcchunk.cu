@@ -942,9 +942,6 @@ void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_
     (void)aadj;
     ck_configure();
     if (g.C < 3) return;
-    // source tiles of whole 64-row M tiles (the transposed pack fills M tiles)
-    const int ntile = ceil_div(g.n, kCkMaxN);
-    const int N = std::min(kCkMaxN, ceil_div(ceil_div(g.n, ntile), 64) * 64);
     ChunkParams p = base_params(co, g, b);
     const size_t sfl = tc_chunk_state_floats(co.ny);
     p.apack = afwd;
@@ -953,7 +950,9 @@ void tc_chunk_prepare(const Coefs<float2> &co, const uint8_t *afwd, const uint8_
         set_bounds(p, g.C, false, half);
         uint8_t *lp = lpack_of(g, b.lpack, false, half, g.page_bytes);
         uint8_t *lph = lpack_of(g, b.lpack, true, 1 - half, g.page_bytes);
-        for (int s0 = 0; s0 < g.n; s0 += N) {
+        for (int s0 = 0, N = 0; s0 < g.n; s0 += N) {
+            // source tiles of whole 64-row M tiles (the transposed pack fills M tiles)
+            N = std::min(kCkMaxN, ceil_div(g.n - s0, 64) * 64);
             p.s0 = s0;
             p.s_end = std::min(g.n, s0 + N);
             p.N = N;
