@@ -35,9 +35,13 @@
 //     B = complex columns of Z packed per (112-column tile, K chunk).
 // Grid: 64-row tiles x 112-column tiles x ks K slices, one CTA per SM,
 // launched cooperatively; operands stream through a shared-memory ring with
-// cp.async.bulk; each CTA's TF32 partial tile goes to L2 and, after a grid
-// barrier, the CTAs of a tile each sum one row slice in rank order and
-// write the epilogue (R in B layout, or X in A, B and fp32 layouts).
+// cp.async.bulk.  The ks CTAs of a tile form one thread-block cluster: each
+// keeps its TF32 partial tile in its own shared memory and, after a bounded
+// cluster barrier, each sums one row slice of the tile from the cluster's
+// shared memory in rank order and writes the epilogue (R in B layout, or X
+// in A and B layouts and into its resident slice).  A solver confined to a
+// partition of the SMs runs the same kernel without clusters: partials
+// through L2, a grid barrier after every GEMM.
 #include <algorithm>
 #include <atomic>
 #include <cstdlib>
