@@ -107,9 +107,10 @@ __device__ __forceinline__ bool on_ring(int y, int x, int ny, int nx) {
 
 // One thread per grid point of a 32 x 8 tile, all sources in order (the sum
 // over s is the same at every point on every run).  The lambda tile with its
-// one-point halo is double-buffered in shared memory: the next source's
-// halo values and field value are loaded into registers while the current
-// source is computed, so each source costs one barrier and no exposed load.
+// one-point halo is double-buffered in shared memory; the halo values and
+// field value of the source two ahead are loaded into registers while the
+// current source is computed, so each source costs one barrier and its loads
+// have two sources' time to land.
 __global__ void __launch_bounds__(TY * TX) gradient_kernel(const float2 *u, const float2 *lam, const double2 *mult,
                                                            const double2 *scale, int ny, int nx, int nb, double d,
                                                            double e, double *grad) {
@@ -142,29 +143,34 @@ __global__ void __launch_bounds__(TY * TX) gradient_kernel(const float2 *u, cons
                                                                                  : -1;
     }
     const size_t fs = (size_t)ny * nx;
-    float2 hv[kPer], uv = make_float2(0.f, 0.f);
-    auto fetch = [&](int s) {
+    // two register sets: the next source (stashed after this one's
+    // arithmetic) and the one after it (loading meanwhile)
+    float2 hA[kPer], hB[kPer], uA = make_float2(0.f, 0.f), uB = make_float2(0.f, 0.f);
+    auto fetch = [&](int s, float2 (&hv)[kPer], float2 &uv) {
 #pragma unroll
         for (int k = 0; k < kPer; ++k)
             hv[k] = hoff[k] >= 0 ? lam[fs * s + (size_t)hoff[k]] : make_float2(0.f, 0.f);
         uv = inside ? u[fs * s + idx] : make_float2(0.f, 0.f);
     };
-    auto stash = [&](int buf) {
+    auto stash = [&](int buf, const float2 (&hv)[kPer]) {
         float2 *Lb = &L[buf][0][0];
 #pragma unroll
         for (int k = 0; k < kPer; ++k)
             if (hl[k] >= 0) Lb[hl[k]] = hv[k];
     };
     double acc = 0;
+    float2 ucur = make_float2(0.f, 0.f);
     if (nb > 0) {
-        fetch(0);
-        stash(0);
+        fetch(0, hA, uA);
+        stash(0, hA);
+        ucur = uA;
     }
-    float2 ucur = uv;
+    if (nb > 1) fetch(1, hB, uB);
     __syncthreads();
-    for (int s = 0; s < nb; ++s) {
+    // source s from L[s & 1]; hn/un hold source s+1, hf/uf take source s+2
+    auto body = [&](int s, const float2 (&hn)[kPer], const float2 &un, float2 (&hf)[kPer], float2 &uf) {
         const int cur = s & 1;
-        if (s + 1 < nb) fetch(s + 1);               // in flight during this source's arithmetic
+        if (s + 2 < nb) fetch(s + 2, hf, uf);       // in flight during two sources' arithmetic
         if (inside) {
             double2 ml = make_double2(0.0, 0.0);
 #pragma unroll
@@ -179,10 +185,14 @@ __global__ void __launch_bounds__(TY * TX) gradient_kernel(const float2 *u, cons
             acc -= av.x * ml.x + av.y * ml.y;    // -Re(conj(av) * ml)
         }
         if (s + 1 < nb) {
-            stash(cur ^ 1);                         // last read in the previous source, before its barrier
-            ucur = uv;
+            stash(cur ^ 1, hn);                     // last read in the previous source, before its barrier
+            ucur = un;
         }
         __syncthreads();
+    };
+    for (int s = 0; s < nb; s += 2) {
+        body(s, hB, uB, hA, uA);
+        if (s + 1 < nb) body(s + 1, hA, uA, hB, uB);
     }
     if (inside) grad[idx] += acc;
 }
